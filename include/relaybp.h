@@ -1,0 +1,156 @@
+/*
+ * relaybp.h - C ABI of the B200-native Relay-BP-S decoder (librelaybp.so).
+ *
+ * Plain C: opaque handles, plain pointers, sizes and int status codes.  No C++
+ * exception crosses this boundary and no torch type appears in it.  Device
+ * buffers passed to rbp_decode are allocated and owned by the caller (e.g. a
+ * torch tensor's data pointer); the library owns only the device copies made
+ * at create time (graph, priors, gamma tables) and a 4-byte work-queue counter
+ * per decoder.  The stream argument is a cudaStream_t passed as void*.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the quantum-supercomputing/pelagos tree).
+ *
+ * Thread safety: a decoder may be used from one host thread at a time; two
+ * decoders are independent.  Error strings are kept per host thread.
+ */
+#ifndef RELAYBP_H_
+#define RELAYBP_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RBP_API __attribute__((visibility("default")))
+#else
+#define RBP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define RBP_OK 0
+#define RBP_ERR_ARGUMENT 1     /* invalid argument; see rbp_last_error() */
+#define RBP_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define RBP_ERR_UNSUPPORTED 3  /* problem outside this build's limits (sizes, degrees) */
+
+/* message storage types; posteriors and memory accumulate in f32 (f64 for F64) */
+#define RBP_MSG_F32 0
+#define RBP_MSG_F16 1
+#define RBP_MSG_BF16 2
+#define RBP_MSG_F64 3
+
+/* rounding of the memory mix  (1 - g) * llr + g * posterior */
+#define RBP_MIX_SEPARATE 0     /* every product and sum rounded once */
+#define RBP_MIX_FMA_GP 1       /* fma(g, posterior, (1 - g) * llr) */
+#define RBP_MIX_FMA_LP 2       /* fma(1 - g, llr, g * posterior) */
+
+typedef struct rbp_graph rbp_graph;
+typedef struct rbp_decoder rbp_decoder;
+
+/* Last error message of the calling host thread ("" when none). */
+RBP_API const char* rbp_last_error(void);
+
+/* Library version string. */
+RBP_API const char* rbp_version(void);
+
+/*
+ * Tanner graph in the reference's edge-centric form, copied to `device`.
+ * Replaces CSRGraph(H_csr, device) and _build_edge_representation
+ * (src/pelagos/graph.py:31-211): edge e is the e-th nonzero of the CSR matrix,
+ * chk_ptr[C+1] delimits each check's edges, edge_var[E] is the variable of
+ * each edge, and var_edges[var_ptr[v]..var_ptr[v+1]) lists variable v's edges
+ * in the order their check messages are summed (graph.py:145 argsort order).
+ * All arrays are host memory.
+ */
+RBP_API int rbp_graph_create(int32_t C, int32_t V, int32_t E,
+                     const int32_t* chk_ptr, const int32_t* edge_var,
+                     const int32_t* var_ptr, const int32_t* var_edges,
+                     int32_t device, rbp_graph** out);
+RBP_API int rbp_graph_destroy(rbp_graph* g);
+
+/* Decode parameters: the RelayBPDecoder constructor arguments that reach the
+ * decode loop (src/pelagos/decoder.py:271-307). */
+typedef struct {
+  int32_t pre_iter;         /* first-phase iterations (ordered memory) */
+  int32_t num_sets;         /* relay legs */
+  int32_t set_max_iter;     /* iterations per relay leg */
+  int32_t stop_nconv;       /* solutions a shot collects before it stops */
+  int32_t msg_type;         /* RBP_MSG_* */
+  int32_t last_leg;         /* 1: unconverged shots return the final hard decision */
+  int32_t use_alpha;        /* normalized min-sum with per-iteration alpha table */
+  int32_t use_beta;         /* offset min-sum */
+  float beta;
+  int32_t mix_mode;         /* RBP_MIX_* */
+} rbp_params;
+
+/*
+ * Decoder: graph + parameters + device copies of the prior LLRs [V], the
+ * leg memory-strength table [num_sets, V] (row l = relay leg l) and the
+ * per-iteration alpha table [n_alpha].  Replaces RelayBPDecoder.__init__
+ * (src/pelagos/decoder.py:271-784) from the graph build onward; the gamma
+ * table stands for the per-leg draws of decoder.py:3684-3700.
+ * llr, gamma_legs and alpha are host memory; gamma_legs may be NULL when
+ * num_sets == 0 and alpha may be NULL when use_alpha == 0.
+ */
+RBP_API int rbp_decoder_create(const rbp_graph* g, const rbp_params* p,
+                       const float* llr, const float* gamma_legs,
+                       const float* alpha, int32_t n_alpha, rbp_decoder** out);
+RBP_API int rbp_decoder_destroy(rbp_decoder* d);
+
+/* Replace the shared prior LLRs (and the selection weights derived from
+ * them) for later decodes; host memory [V].  Replaces
+ * RelayBPDecoder.override_llr_columns (src/pelagos/decoder.py:785-834). */
+RBP_API int rbp_decoder_set_llr(rbp_decoder* d, const float* llr);
+
+/* Launch shape: `group_threads` threads decode one shot at a time (a
+ * multiple of 32, at most 1024) and a thread block holds `groups_per_block`
+ * such groups.  0/0 picks a default.  Fails with RBP_ERR_UNSUPPORTED when the
+ * shape's shared memory does not fit. */
+RBP_API int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block);
+
+/* Shared-memory bytes of one group and of the block-wide tables for the
+ * current message type; the shape currently configured. */
+RBP_API int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem,
+                      int32_t* group_threads, int32_t* groups_per_block, int32_t* blocks);
+
+/* Per-call inputs (device memory).  Optional pointers may be NULL.
+ * Mirrors decode()'s keyword arguments (src/pelagos/decoder.py:2317-2361). */
+typedef struct {
+  const uint8_t* syndromes;        /* [B, C] bits in the low bit of each byte */
+  const float* llr_per_shot;       /* [B, V] prior_llr, overrides the shared LLRs */
+  const float* gamma_pre;          /* [B, V] init_gamma for the first phase */
+  float gamma0;                    /* first-phase strength when gamma_pre is NULL (0 for algo=plain) */
+  const float* init_posterior;     /* [B, V] posterior the first phase starts from */
+  const float* gamma_legs_shot;    /* [B, n_shot_legs, V] per-shot strengths of legs < n_shot_legs */
+  int32_t n_shot_legs;
+  int32_t pre_iter;                /* first-phase iterations for this call (pre_iter_override) */
+  int32_t skip_relay_legs;         /* 1: stop after the first phase */
+} rbp_batch;
+
+/* Outputs (device memory).  Any may be NULL except found_count/iterations. */
+typedef struct {
+  uint8_t* errors;                 /* [B, V] 0/1 */
+  uint32_t* errors_packed;         /* [B, ceil(V/32)] bit v%32 of word v/32 */
+  float* weights;                  /* [B] selected solution weight, +inf when none */
+  int64_t* weight_fixed;           /* [B] exact weight in units of 2^-32, INT64_MAX when none */
+  int32_t* found_count;            /* [B] solutions found */
+  int32_t* iterations;             /* [B] BP iterations the shot ran */
+  void* last_posterior;            /* [B, V] f32 (f64 for RBP_MSG_F64) posterior at the end */
+} rbp_outputs;
+
+/*
+ * Decode B shots on `stream`.  Asynchronous: returns after the launch.
+ * Replaces RelayBPDecoder.decode (src/pelagos/decoder.py:2317-2449) and its
+ * single-GPU loop _decode_loop_single_gpu (decoder.py:3394-3873) with all its
+ * per-iteration kernels (src/pelagos/kernels.py:609-1350).
+ */
+RBP_API int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs* out,
+               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RELAYBP_H_ */

@@ -1,0 +1,551 @@
+"""RelayBPDecoder: drop-in host interface over the sm_100a Relay-BP-S kernel.
+
+Mirrors the reference class ``RelayBPDecoder`` (src/pelagos/decoder.py:247-3891):
+same constructor arguments, the same argument validation and error types, and
+``decode(syndromes, ...)`` returning a dict with the same keys.  All decoding
+runs in one persistent CUDA kernel per call (pelagos_b200/csrc/relaybp.cu)
+reached through the C ABI of include/relaybp.h; there is no CPU path.
+
+Differences from the reference, by design:
+
+* message precision: ``data_type`` "float16" / "bfloat16" store messages in
+  16 bits while posteriors, memory and sums stay float32 (the reference keeps
+  everything in float16 for "float16");
+* solution weights are exact (64-bit fixed point, 2^-32 units), so the
+  lowest-weight selection does not depend on a summation order;
+* results are fresh tensors (the reference returns views of per-batch-size
+  cached buffers that the next decode overwrites);
+* ``scheduling="layered"`` and ``fast_max_unconverged_pct`` are not provided
+  (they need leg-synchronous batches; the kernel retires each shot on its own).
+"""
+
+from __future__ import annotations
+
+from typing import Dict, List, Optional, Sequence, Tuple, Union
+
+import ctypes as ct
+import numpy as np
+import torch
+from scipy.sparse import csr_matrix
+
+from . import _native as nat
+from .graph import TannerGraph
+from .utils import (
+    GAMMA_DRAW_MODES,
+    alpha_schedule,
+    compute_log_prior_ratios,
+    sample_gamma_per_variable,
+    sample_gamma_uniform,
+    validate_csr_matrix,
+    validate_error_priors,
+)
+
+#: Values accepted by ``unconverged_correction`` (decoder.py:222-223).
+UNCONVERGED_CORRECTIONS = ("first_leg", "last_leg")
+
+_DTYPE_ALIASES = {
+    "float": "float32",
+    "half": "float16",
+    "double": "float64",
+    "fp16": "float16",
+    "fp32": "float32",
+    "fp64": "float64",
+    "bf16": "bfloat16",
+}
+_MSG_TYPES = {
+    "float32": nat.RBP_MSG_F32,
+    "float16": nat.RBP_MSG_F16,
+    "bfloat16": nat.RBP_MSG_BF16,
+    "float64": nat.RBP_MSG_F64,
+}
+_MIX_MODES = {"separate": nat.RBP_MIX_SEPARATE, "fma_gp": nat.RBP_MIX_FMA_GP, "fma_lp": nat.RBP_MIX_FMA_LP}
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return ct.c_void_p(t.data_ptr()) if t is not None else ct.c_void_p(0)
+
+
+class _NativeDecoder:
+    """Owns one device's rbp_graph + rbp_decoder handles."""
+
+    def __init__(self, graph: TannerGraph, device: int, params: nat.RbpParams, llr: np.ndarray,
+                 gamma_legs: np.ndarray, alpha: np.ndarray):
+        L = nat.lib()
+        self.device = device
+        self._graph = ct.c_void_p()
+        self._dec = ct.c_void_p()
+        nat.check(L.rbp_graph_create(graph.C, graph.V, graph.E, nat.i32_ptr(graph.chk_ptr),
+                                     nat.i32_ptr(graph.edge_var), nat.i32_ptr(graph.var_ptr),
+                                     nat.i32_ptr(graph.var_edges), device, ct.byref(self._graph)),
+                  "rbp_graph_create")
+        llr = np.ascontiguousarray(llr, dtype=np.float32)
+        gamma_legs = np.ascontiguousarray(gamma_legs, dtype=np.float32)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float32)
+        rc = L.rbp_decoder_create(self._graph, ct.byref(params), nat.f32_ptr(llr),
+                                  nat.f32_ptr(gamma_legs) if gamma_legs.size else None,
+                                  nat.f32_ptr(alpha), int(alpha.size), ct.byref(self._dec))
+        if rc != nat.RBP_OK:
+            L.rbp_graph_destroy(self._graph)
+            self._graph = ct.c_void_p()
+        nat.check(rc, "rbp_decoder_create")
+
+    def set_llr(self, llr: np.ndarray):
+        llr = np.ascontiguousarray(llr, dtype=np.float32)
+        nat.check(nat.lib().rbp_decoder_set_llr(self._dec, nat.f32_ptr(llr)), "rbp_decoder_set_llr")
+
+    def configure(self, group_threads: int, groups_per_block: int):
+        nat.check(nat.lib().rbp_decoder_configure(self._dec, int(group_threads), int(groups_per_block)),
+                  "rbp_decoder_configure")
+
+    def query(self) -> dict:
+        gs, bs = ct.c_int64(), ct.c_int64()
+        gt, gb, nb = ct.c_int32(), ct.c_int32(), ct.c_int32()
+        nat.check(nat.lib().rbp_decoder_query(self._dec, ct.byref(gs), ct.byref(bs), ct.byref(gt),
+                                              ct.byref(gb), ct.byref(nb)), "rbp_decoder_query")
+        return {"group_smem": gs.value, "block_smem": bs.value, "group_threads": gt.value,
+                "groups_per_block": gb.value, "blocks": nb.value}
+
+    def decode(self, B: int, batch: nat.RbpBatch, outs: nat.RbpOutputs, stream: int):
+        nat.check(nat.lib().rbp_decode(self._dec, int(B), ct.byref(batch), ct.byref(outs),
+                                       ct.c_void_p(stream)), "rbp_decode")
+
+    def close(self):
+        if getattr(self, "_dec", None):
+            nat.lib().rbp_decoder_destroy(self._dec)
+            self._dec = ct.c_void_p()
+        if getattr(self, "_graph", None):
+            nat.lib().rbp_graph_destroy(self._graph)
+            self._graph = ct.c_void_p()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RelayBPDecoder:
+    """Relay-BP-S decoder on one (or, as independent replicas, several) B200 GPUs.
+
+    Constructor arguments and their validation follow decoder.py:271-784.
+    Extra keyword arguments of this implementation:
+
+    * ``mix_rounding``: rounding of the memory mix (1-g)*llr + g*posterior:
+      "separate" (default; one rounding per operation), "fma_gp" or "fma_lp";
+    * ``launch``: optional (group_threads, groups_per_block) kernel shape.
+    """
+
+    def __init__(
+        self,
+        H_csr: csr_matrix,
+        error_priors: np.ndarray,
+        pre_iter: int = 80,
+        num_sets: int = 100,
+        set_max_iter: int = 60,
+        gamma0: float = 0.65,
+        gamma_dist_interval: Tuple[float, float] = (-0.24, 0.66),
+        stop_nconv: int = 5,
+        normalized_min_sum_alpha: Optional[float] = None,
+        offset_min_sum_beta: Optional[float] = None,
+        data_type: str = "float32",
+        device: Union[str, List[int], int] = [0],  # noqa: B006 - reference default
+        seed: int = 1234,
+        gamma_draw: str = "broadcast",
+        bitpack_output: bool = False,
+        algo: Optional[str] = None,
+        perf: Optional[str] = None,
+        alpha_iteration_scaling_factor: Optional[float] = 1.0,
+        explicit_gammas: Optional[np.ndarray] = None,
+        gamma_dist_interval_by_error: Optional[np.ndarray] = None,
+        fast_max_unconverged_pct: Optional[float] = None,
+        scheduling: str = "flood-fill",
+        layered_k_iters: int = 0,
+        layered_block_policy: str = "contiguous",
+        layered_num_blocks: Optional[int] = None,
+        layered_target_edges_per_block: Optional[int] = None,
+        layered_block_seed: int = 42,
+        unconverged_correction: str = "first_leg",
+        *,
+        mix_rounding: str = "separate",
+        launch: Optional[Tuple[int, int]] = None,
+    ):
+        if unconverged_correction not in UNCONVERGED_CORRECTIONS:
+            raise ValueError(
+                f"unconverged_correction must be one of {UNCONVERGED_CORRECTIONS} "
+                f"(got {unconverged_correction!r})")
+        self.unconverged_correction = unconverged_correction
+        validate_csr_matrix(H_csr)
+        error_priors = validate_error_priors(error_priors)
+        if normalized_min_sum_alpha is not None and offset_min_sum_beta is not None:
+            raise ValueError("Cannot specify both normalized_min_sum_alpha and offset_min_sum_beta")
+        if normalized_min_sum_alpha is not None and not (0 <= normalized_min_sum_alpha <= 1):
+            raise ValueError("normalized_min_sum_alpha must be in [0, 1]")
+        if offset_min_sum_beta is not None and offset_min_sum_beta < 0:
+            raise ValueError("offset_min_sum_beta must be >= 0")
+        self.H_csr = H_csr
+        self.check_permutation = None
+        self.error_priors = error_priors
+        self.pre_iter = int(pre_iter)
+        self.num_sets = int(num_sets)
+        self.set_max_iter = int(set_max_iter)
+        self.gamma0 = gamma0
+        self.gamma_dist_interval = gamma_dist_interval
+        self.stop_nconv = int(stop_nconv)
+        if fast_max_unconverged_pct is not None:
+            if not (0.0 <= fast_max_unconverged_pct <= 1.0):
+                raise ValueError(
+                    f"fast_max_unconverged_pct must be between 0.0 and 1.0, got {fast_max_unconverged_pct}")
+            raise NotImplementedError(
+                "fast_max_unconverged_pct needs leg-synchronous batches; this decoder retires each shot "
+                "independently inside one kernel")
+        self.fast_max_unconverged_pct = None
+        self.normalized_min_sum_alpha = normalized_min_sum_alpha
+        self.offset_min_sum_beta = offset_min_sum_beta
+
+        data_type = _DTYPE_ALIASES.get(data_type, data_type)
+        if data_type not in _MSG_TYPES:
+            raise ValueError(
+                f"data_type must be 'float16', 'bfloat16', 'float32', or 'float64', got {data_type}")
+        self.dtype_str = data_type
+        self.dtype = {"float16": torch.float16, "bfloat16": torch.bfloat16, "float32": torch.float32,
+                      "float64": torch.float64}[data_type]
+        self._acc_dtype = torch.float64 if data_type == "float64" else torch.float32
+        self.device_ids = self._parse_device_spec(device)
+        self.num_gpus = len(self.device_ids)
+        if not torch.cuda.is_available():
+            raise RuntimeError("GPU not available (install a GPU-enabled PyTorch build: CUDA or ROCm)")
+        self.device_type = "cuda"
+        self._device_strs = {g: f"cuda:{g}" for g in self.device_ids}
+        self.seed = int(seed)
+        if gamma_draw not in GAMMA_DRAW_MODES:
+            raise ValueError(f"gamma_draw must be one of {GAMMA_DRAW_MODES}; got {gamma_draw!r}")
+        self.gamma_draw = gamma_draw
+        self.bitpack_output = bool(bitpack_output)
+        if algo not in ("relay", "plain"):
+            raise ValueError(f"Unknown algo '{algo}'. Use 'relay' or 'plain'.")
+        self.algo = algo
+        perf_norm = (perf or "throughput").strip().lower()
+        perf_aliases = {"default": "default", "row": "default", "rowwise": "default",
+                        "throughput": "throughput", "btile": "throughput"}
+        if perf_norm not in perf_aliases:
+            raise ValueError(f"Unknown perf '{perf_norm}'. Use 'default'/'throughput'.")
+        self.perf = perf_aliases[perf_norm]
+        self.alpha_iteration_scaling_factor = float(alpha_iteration_scaling_factor or 1.0)
+        scheduling_norm = (scheduling or "flood-fill").strip().lower()
+        if scheduling_norm not in ("flood-fill", "layered"):
+            raise ValueError(f"Unknown scheduling '{scheduling_norm}'. Use 'flood-fill' or 'layered'.")
+        if scheduling_norm == "layered" and self.perf != "throughput":
+            raise ValueError("scheduling='layered' requires perf='throughput'")
+        if scheduling_norm == "layered":
+            raise NotImplementedError("scheduling='layered' is not provided; use 'flood-fill'")
+        self.scheduling = scheduling_norm
+        if mix_rounding not in _MIX_MODES:
+            raise ValueError(f"mix_rounding must be one of {tuple(_MIX_MODES)}")
+        self.mix_rounding = mix_rounding
+
+        V = int(H_csr.shape[1])
+        self._explicit_gammas = None
+        if explicit_gammas is not None:
+            eg = np.asarray(explicit_gammas, dtype=np.float32)
+            if eg.ndim != 2 or eg.shape[1] != V:
+                raise ValueError(f"explicit_gammas must have shape (K, V={V})")
+            self._explicit_gammas = eg
+        self._gamma_by_error = None
+        if gamma_dist_interval_by_error is not None:
+            gd = np.asarray(gamma_dist_interval_by_error, dtype=np.float32)
+            if gd.ndim != 2 or gd.shape[0] != V or gd.shape[1] != 2:
+                raise ValueError(
+                    f"gamma_dist_interval_by_error must have shape (V={V}, 2), got {tuple(gd.shape)}")
+            if np.any(gd[:, 0] > gd[:, 1]):
+                raise ValueError("gamma_dist_interval_by_error: lower bounds must be <= upper bounds")
+            self._gamma_by_error = gd
+
+        self.graph = TannerGraph(H_csr)
+        self.C, self.V, self.E = self.graph.C, self.graph.V, self.graph.E
+        self.log_prior_ratios = compute_log_prior_ratios(error_priors)          # [V] f32
+        self.wj = np.where(np.isfinite(self.log_prior_ratios), self.log_prior_ratios, 0).astype(np.float32)
+        # The reference seeds the global torch RNG here (decoder.py:774).
+        torch.manual_seed(seed)
+
+        self._launch = tuple(launch) if launch is not None else None
+        self._native: Dict[int, _NativeDecoder] = {}
+        self._legs_broadcast: Dict[int, torch.Tensor] = {}
+        self._alpha_len = max(self.pre_iter, self.set_max_iter, 1)
+        for g in self.device_ids:
+            self._native[g] = self._make_native(g, self._alpha_len)
+
+    # ------------------------------------------------------------------ construction helpers
+
+    def _parse_device_spec(self, device) -> List[int]:
+        """decoder.py:1403-1452."""
+        if isinstance(device, int):
+            if device < 1:
+                raise ValueError(f"Number of GPUs must be >= 1, got {device}")
+            available = torch.cuda.device_count()
+            if device > available:
+                raise ValueError(f"Requested {device} GPUs but only {available} available")
+            return list(range(device))
+        if isinstance(device, list):
+            if not device:
+                raise ValueError("Device list cannot be empty")
+            available = torch.cuda.device_count()
+            for gpu_id in device:
+                if not isinstance(gpu_id, int):
+                    raise ValueError(f"Device IDs must be integers, got {type(gpu_id)}")
+                if gpu_id < 0 or gpu_id >= available:
+                    raise ValueError(f"Device ID {gpu_id} out of range [0, {available - 1}]")
+            return list(device)
+        if isinstance(device, str):
+            if device.strip().lower() in ("auto", "cuda", "rocm"):
+                return [0]
+            raise ValueError(f"Unsupported device string '{device}'. Use List[int], int, or 'auto'/'cuda'.")
+        raise ValueError(f"Invalid device type: {type(device)}. Expected List[int], int, or str.")
+
+    def _leg_table(self, gpu_id: int) -> np.ndarray:
+        """[num_sets, V] memory strengths of the relay legs with broadcast draws (decoder.py:3684-3700)."""
+        R, V = self.num_sets, self.V
+        if R == 0:
+            return np.zeros((0, V), np.float32)
+        if self._explicit_gammas is not None:
+            K = self._explicit_gammas.shape[0]
+            return np.stack([self._explicit_gammas[(leg + 1) % K] for leg in range(R)]).astype(np.float32)
+        dev = self._device_strs[gpu_id]
+        rows = []
+        if self._gamma_by_error is not None:
+            iv = torch.from_numpy(self._gamma_by_error).to(dev)
+            for leg in range(R):
+                rows.append(sample_gamma_per_variable(1, V, iv, dev, self.seed + leg))
+        else:
+            lo, hi = self.gamma_dist_interval
+            for leg in range(R):
+                rows.append(sample_gamma_uniform(1, V, lo, hi, dev, self.seed + leg))
+        return torch.cat(rows, 0).float().cpu().numpy()
+
+    def _per_row_legs(self, B: int, gpu_id: int, row0: int) -> torch.Tensor:
+        """[B, num_sets, V] per-shot leg strengths for gamma_draw='per_row' (rows row0..row0+B of each draw)."""
+        dev = self._device_strs[gpu_id]
+        total = row0 + B
+        out = torch.empty(B, self.num_sets, self.V, dtype=torch.float32, device=dev)
+        for leg in range(self.num_sets):
+            if self._gamma_by_error is not None:
+                iv = torch.from_numpy(self._gamma_by_error).to(dev)
+                g = sample_gamma_per_variable(total, self.V, iv, dev, self.seed + leg)
+            else:
+                lo, hi = self.gamma_dist_interval
+                g = sample_gamma_uniform(total, self.V, lo, hi, dev, self.seed + leg)
+            out[:, leg, :] = g[row0:total].float()
+        return out
+
+    def _params(self) -> nat.RbpParams:
+        use_alpha, _ = alpha_schedule(self.normalized_min_sum_alpha, self.alpha_iteration_scaling_factor, 1)
+        return nat.RbpParams(
+            pre_iter=self.pre_iter, num_sets=self.num_sets, set_max_iter=self.set_max_iter,
+            stop_nconv=self.stop_nconv, msg_type=_MSG_TYPES[self.dtype_str],
+            last_leg=1 if self.unconverged_correction == "last_leg" else 0,
+            use_alpha=1 if use_alpha else 0,
+            use_beta=1 if self.offset_min_sum_beta is not None else 0,
+            beta=float(self.offset_min_sum_beta or 0.0), mix_mode=_MIX_MODES[self.mix_rounding])
+
+    def _make_native(self, gpu_id: int, alpha_len: int) -> _NativeDecoder:
+        _, alpha = alpha_schedule(self.normalized_min_sum_alpha, self.alpha_iteration_scaling_factor, alpha_len)
+        with torch.cuda.device(gpu_id):
+            nd = _NativeDecoder(self.graph, gpu_id, self._params(), self.log_prior_ratios,
+                                self._leg_table(gpu_id), alpha)
+            if self._launch is not None:
+                nd.configure(*self._launch)
+        return nd
+
+    # ------------------------------------------------------------------ public helpers
+
+    def configure_launch(self, group_threads: int, groups_per_block: int) -> None:
+        """Set the kernel shape (threads per shot group, groups per thread block)."""
+        self._launch = (int(group_threads), int(groups_per_block))
+        for nd in self._native.values():
+            nd.configure(*self._launch)
+
+    def launch_info(self) -> dict:
+        return self._native[self.device_ids[0]].query()
+
+    def override_llr_columns(self, cols, value):
+        """Overwrite prior LLRs (and selection weights) of some columns; returns a restore callable.
+
+        decoder.py:786-834.  Values bypass the prior clipping, so negative LLRs are allowed.
+        """
+        cols = np.asarray(cols, dtype=np.int64)
+        saved_llr = self.log_prior_ratios[cols].copy()
+        saved_wj = self.wj[cols].copy()
+        self.log_prior_ratios[cols] = np.asarray(value, dtype=np.float32)
+        self.wj[cols] = np.asarray(value, dtype=np.float32)
+        self._push_llr()
+
+        def _restore():
+            self.log_prior_ratios[cols] = saved_llr
+            self.wj[cols] = saved_wj
+            self._push_llr()
+
+        return _restore
+
+    def _push_llr(self):
+        for nd in self._native.values():
+            nd.set_llr(self.log_prior_ratios)
+
+    def get_stats(self) -> Dict:
+        return {
+            "graph": self.graph.get_stats(),
+            "parameters": {
+                "pre_iter": self.pre_iter, "num_sets": self.num_sets, "set_max_iter": self.set_max_iter,
+                "gamma0": self.gamma0, "gamma_dist_interval": self.gamma_dist_interval,
+                "stop_nconv": self.stop_nconv, "dtype": self.dtype_str, "device": self.device_ids,
+                "algo": self.algo, "perf": self.perf,
+            },
+        }
+
+    # ------------------------------------------------------------------ decode
+
+    def decode(
+        self,
+        syndromes: torch.Tensor,
+        *,
+        init_posterior: Optional[torch.Tensor] = None,
+        init_gamma: Optional[torch.Tensor] = None,
+        skip_relay_legs: bool = False,
+        pre_iter_override: Optional[int] = None,
+        return_last_posterior: bool = False,
+        prior_llr: Optional[torch.Tensor] = None,
+        leg_gammas: Optional[torch.Tensor] = None,
+    ) -> Dict[str, torch.Tensor]:
+        """Decode [B, C] uint8 syndromes; see decoder.py:2317-2361 for the keyword arguments.
+
+        ``leg_gammas`` ([B, L, V], this implementation only) gives each shot its own
+        memory strengths for relay legs 0..L-1; later legs use the seeded table.
+        """
+        if not isinstance(syndromes, torch.Tensor):
+            syndromes = torch.as_tensor(np.asarray(syndromes))
+        if syndromes.ndim != 2:
+            raise ValueError(f"Expected a [B, {self.C}] syndrome tensor, got shape {tuple(syndromes.shape)}")
+        B = int(syndromes.shape[0])
+        if syndromes.shape[1] != self.C:
+            raise ValueError(f"Expected {self.C} syndrome bits, got {syndromes.shape[1]}")
+        advanced = (init_posterior is not None or init_gamma is not None or skip_relay_legs
+                    or pre_iter_override is not None or return_last_posterior or prior_llr is not None)
+        if advanced:
+            if self.perf != "throughput":
+                raise ValueError(
+                    "init_posterior / init_gamma / skip_relay_legs / pre_iter_override / "
+                    f"return_last_posterior are only supported in throughput perf mode (got perf={self.perf!r}).")
+            if self.num_gpus > 1:
+                raise ValueError(
+                    "init_posterior / init_gamma / skip_relay_legs / pre_iter_override / "
+                    "return_last_posterior / prior_llr require single-GPU decode "
+                    f"(self.num_gpus={self.num_gpus}).")
+            for name, t in (("init_posterior", init_posterior), ("init_gamma", init_gamma),
+                            ("prior_llr", prior_llr)):
+                if t is not None and tuple(t.shape) != (B, self.V):
+                    raise ValueError(f"{name} shape {tuple(t.shape)} != ({B}, {self.V})")
+        if leg_gammas is not None and (leg_gammas.ndim != 3 or leg_gammas.shape[0] != B
+                                       or leg_gammas.shape[2] != self.V):
+            raise ValueError(f"leg_gammas must have shape ({B}, L, {self.V})")
+        pre = self.pre_iter if pre_iter_override is None else int(pre_iter_override)
+        if pre < 0:
+            raise ValueError("pre_iter_override must be >= 0")
+        if pre > self._alpha_len and self.normalized_min_sum_alpha is not None:
+            self._alpha_len = pre
+            for g in self.device_ids:
+                self._native[g].close()
+                self._native[g] = self._make_native(g, self._alpha_len)
+
+        if self.num_gpus == 1:
+            return self._decode_on(self.device_ids[0], syndromes, 0, pre, init_posterior, init_gamma,
+                                   skip_relay_legs, return_last_posterior, prior_llr, leg_gammas)
+        splits = self._split_batch(B, self.num_gpus)
+        parts = []
+        for gpu_id, (s0, s1) in zip(self.device_ids, splits):
+            lg = leg_gammas[s0:s1] if leg_gammas is not None else None
+            parts.append(self._decode_on(gpu_id, syndromes[s0:s1], s0, pre, None, None, False, False,
+                                         None, lg))
+        return self._gather(parts, splits)
+
+    @staticmethod
+    def _split_batch(B: int, num_gpus: int) -> List[Tuple[int, int]]:
+        """Contiguous, near-equal shards; the first B % n get one extra shot (decoder.py:2451-2473)."""
+        base, rem = divmod(B, num_gpus)
+        out, start = [], 0
+        for i in range(num_gpus):
+            end = start + base + (1 if i < rem else 0)
+            out.append((start, end))
+            start = end
+        return out
+
+    def _gather(self, parts: Sequence[dict], splits) -> Dict[str, torch.Tensor]:
+        target = self._device_strs[self.device_ids[0]]
+        out = {}
+        for k in ("errors", "weights", "valid_mask", "iterations", "found_count"):
+            out[k] = torch.cat([p[k].to(target) for p in parts], 0)
+        unc = [p["unconverged_indices"].to(target) + s0 for p, (s0, _) in zip(parts, splits)]
+        out["unconverged_indices"] = torch.cat(unc, 0).to(torch.int32)
+        return out
+
+    def _decode_on(self, gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
+                   return_last_posterior, prior_llr, leg_gammas) -> Dict[str, torch.Tensor]:
+        B = int(syndromes.shape[0])
+        dev = self._device_strs[gpu_id]
+        with torch.cuda.device(gpu_id):
+            syn = syndromes.to(device=dev, dtype=torch.uint8).contiguous()
+            f32 = dict(device=dev, dtype=torch.float32)
+            ip = init_posterior.to(**f32).contiguous() if init_posterior is not None else None
+            ig = None
+            gamma0 = 0.0
+            if self.algo == "relay":
+                if init_gamma is not None:
+                    ig = init_gamma.to(**f32).contiguous()
+                else:
+                    gamma0 = float(np.float32(self.gamma0))
+            pl = prior_llr.to(**f32).contiguous() if prior_llr is not None else None
+            shot_legs, n_shot_legs = None, 0
+            if self.gamma_draw == "per_row" and self._explicit_gammas is None and self.num_sets > 0:
+                # each device draws rows 0..B_i-1, as the reference's per-GPU loop does
+                shot_legs = self._per_row_legs(B, gpu_id, 0)
+                n_shot_legs = self.num_sets
+            if leg_gammas is not None:
+                lg = leg_gammas.to(**f32).contiguous()
+                if shot_legs is not None:
+                    shot_legs[:, :lg.shape[1]] = lg[:, :self.num_sets]
+                else:
+                    shot_legs, n_shot_legs = lg, min(int(lg.shape[1]), self.num_sets)
+            W = (self.V + 31) // 32
+            found = torch.empty(B, dtype=torch.int32, device=dev)
+            iters = torch.empty(B, dtype=torch.int32, device=dev)
+            wfix = torch.empty(B, dtype=torch.int64, device=dev)
+            errors = packed = None
+            if self.bitpack_output:
+                packed = torch.empty(B, W, dtype=torch.int32, device=dev)
+            else:
+                errors = torch.empty(B, self.V, dtype=torch.uint8, device=dev)
+            last_post = torch.empty(B, self.V, dtype=self._acc_dtype, device=dev) if return_last_posterior else None
+            batch = nat.RbpBatch(syndromes=_ptr(syn), llr_per_shot=_ptr(pl), gamma_pre=_ptr(ig),
+                                 gamma0=gamma0, init_posterior=_ptr(ip), gamma_legs_shot=_ptr(shot_legs),
+                                 n_shot_legs=n_shot_legs, pre_iter=pre,
+                                 skip_relay_legs=1 if skip_relay_legs else 0)
+            outs = nat.RbpOutputs(errors=_ptr(errors), errors_packed=_ptr(packed), weights=None,
+                                  weight_fixed=_ptr(wfix), found_count=_ptr(found), iterations=_ptr(iters),
+                                  last_posterior=_ptr(last_post))
+            stream = torch.cuda.current_stream(gpu_id).cuda_stream
+            self._native[gpu_id].decode(B, batch, outs, stream)
+            has = wfix != torch.iinfo(torch.int64).max
+            wdt = torch.float64 if self.dtype_str == "float64" else torch.float32
+            weights = torch.where(has, wfix.to(torch.float64) * (2.0 ** -32),
+                                  torch.full_like(wfix, 0, dtype=torch.float64) + float("inf")).to(wdt)
+            result = {
+                "errors": packed if self.bitpack_output else errors,
+                "weights": weights,
+                "valid_mask": found >= self.stop_nconv,
+                "iterations": iters,
+                "found_count": found,
+                "unconverged_indices": torch.nonzero(found < self.stop_nconv).flatten().to(torch.int32),
+                "weight_fixed": wfix,
+            }
+            if return_last_posterior:
+                result["last_posterior"] = last_post
+            # Inputs freed here stay safe: the caching allocator reuses their memory
+            # only for work ordered after this stream's kernel.
+            return result
