@@ -25,6 +25,7 @@ import json
 import os
 import statistics
 import subprocess
+import sys
 import threading
 import time
 
@@ -54,7 +55,7 @@ def _dist():
 
 
 class ClockSampler:
-    """nvidia-smi SM clocks and throttle reasons, sampled every 200 ms in the background."""
+    """nvidia-smi SM clocks and throttle reasons every 200 ms, with host timestamps."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -62,11 +63,10 @@ class ClockSampler:
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
-        self.rows: list[list[str]] = []
-        self._stop = threading.Event()
+        self.rows: list[tuple[float, list[str]]] = []
         self._proc = None
 
-    def __enter__(self):
+    def start(self):
         try:
             self._proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
@@ -79,9 +79,9 @@ class ClockSampler:
 
     def _read(self):
         for line in self._proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.time(), [x.strip() for x in line.split(",")]))
 
-    def __exit__(self, *a):
+    def stop(self):
         if self._proc is not None:
             self._proc.terminate()
             try:
@@ -89,16 +89,25 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self._proc.kill()
 
-    def summary(self) -> dict:
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+    def summary(self, t0: float, t1: float) -> dict:
+        rows = [r for (ts, r) in self.rows if t0 <= ts <= t1 and len(r) > 8]
+        if not rows:  # window shorter than the sampling period: nearest samples
+            rows = [r for (ts, r) in sorted(self.rows, key=lambda x: abs(x[0] - (t0 + t1) / 2))[:2] if len(r) > 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mx = [v for v in (num(r[2]) for r in rows) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4)
-                          if r[5 + i].lower().startswith("active")})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def cpu_baseline(w, syn, legs, seconds: float = 12.0) -> dict:
@@ -142,9 +151,10 @@ def run_reference_arm(args) -> None:
         gen.manual_seed(RELAY["seed"] + leg)
         legs.append((lo + (hi - lo) * torch.rand(1, w.H.shape[1], generator=gen)).numpy())
     legs = np.concatenate(legs).astype(np.float32)
+    per_step = min(args.ref_seconds, 90.0 / max(args.steps, 1))  # whole run within a few minutes
     for _ in range(args.warmup):
-        cpu_baseline(w, syn, legs, seconds=2.0)
-    vals = [cpu_baseline(w, syn, legs, seconds=args.ref_seconds) for _ in range(args.steps)]
+        cpu_baseline(w, syn, legs, seconds=1.0)
+    vals = [cpu_baseline(w, syn, legs, seconds=per_step) for _ in range(args.steps)]
     v = float(np.mean([x["value"] for x in vals]))
     base = vals[-1]
     line = {
@@ -165,7 +175,7 @@ def run_reference_arm(args) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--dtype", default="float32")
@@ -207,6 +217,7 @@ def main():
             pg.barrier()
         torch.cuda.synchronize()
 
+    clocks = ClockSampler(local).start()
     # warm-up (untimed)
     out = None
     for _ in range(args.warmup):
@@ -215,28 +226,30 @@ def main():
     torch.cuda.synchronize()
 
     # ---------------- device-resident timing: K steps in one bracket
-    kern_ms = []
     iters_total = 0
-    with ClockSampler(local) as clocks:
-        barrier()
-        t_start = torch.cuda.Event(enable_timing=True)
-        t_end = torch.cuda.Event(enable_timing=True)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-        t_start.record(stream)
-        outs = []
-        for k in range(args.steps):
-            flush.zero_()
-            ev[k][0].record(stream)
-            o = dec.decode(syn_dev)
-            ev[k][1].record(stream)
-            outs.append(o)
-        t_end.record(stream)
-        barrier()
+    barrier()
+    wall0 = time.time()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start.record(stream)
+    step_iters = []
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        o = dec.decode(syn_dev)
+        ev[k][1].record(stream)
+        step_iters.append(o["iterations"])
+        out = o
+    t_end.record(stream)
+    barrier()
+    wall1 = time.time()
+    clocks.stop()
     total_ms = t_start.elapsed_time(t_end)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
-    for o in outs:
-        iters_total += int(o["iterations"].sum().item())
+    for it in step_iters:
+        iters_total += int(it.sum().item())
+    print("per-step ms: " + " ".join(f"{x:.2f}" for x in kern_ms), file=sys.stderr)
     ms_step = total_ms / args.steps
     if pg is not None:
         t = torch.tensor([ms_step], device=dev)
@@ -273,7 +286,7 @@ def main():
     e2e_value = world * shots / (e2e_ms / 1000.0)
 
     if rank == 0:
-        last = {k: v.cpu().numpy() for k, v in outs[-1].items() if isinstance(v, torch.Tensor)}
+        last = {k: v.cpu().numpy() for k, v in out.items() if isinstance(v, torch.Tensor)}
         conv = last["found_count"] > 0
         fails = w.logical_failures(err, last["errors"], conv)
         ler = float(fails.mean())
@@ -284,7 +297,7 @@ def main():
         kern = float(np.mean(kern_ms))
         achieved = bps * (iters_total / args.steps) / (kern / 1000.0) / 1e9
         peaks = _peaks()
-        clk = clocks.summary()
+        clk = clocks.summary(wall0, wall1)
         sm_ghz = (clk["sm_mhz"] or 1965.0) / 1000.0
         smem_peak = torch.cuda.get_device_properties(local).multi_processor_count * 128 * sm_ghz
         line = {

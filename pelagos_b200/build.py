@@ -35,17 +35,36 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu"))
 
 
-def native_cmd(out: Path = OUT) -> list[str]:
+def _compile_cmd(src: Path, obj: Path) -> list[str]:
     return [nvcc(), *ARCH, "-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-            "-Xcompiler", "-fvisibility=hidden", "-shared", "-cudart", "static",
-            f"-I{ROOT / 'include'}", "-o", str(out), *map(str, sources())]
+            "-Xcompiler", "-fvisibility=hidden", f"-I{ROOT / 'include'}", "-c", "-o", str(obj), str(src)]
+
+
+def native_cmd(out: Path = OUT) -> list[str]:
+    """Link step (after every source is compiled to an object next to `out`)."""
+    objs = [str(out.parent / (s.stem + ".o")) for s in sources()]
+    return [nvcc(), *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fvisibility=hidden",
+            "-o", str(out), *objs]
 
 
 def build_native(force: bool = False, verbose: bool = True) -> Path:
+    """Compile the sources in parallel (one nvcc per file), then link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
+
     OUT.parent.mkdir(parents=True, exist_ok=True)
     deps = sources() + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "relaybp.h", Path(__file__)]
     if not force and OUT.exists() and all(OUT.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return OUT
+    jobs = [(s, OUT.parent / (s.stem + ".o")) for s in sources()]
+
+    def run(job):
+        cmd = _compile_cmd(*job)
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        list(ex.map(run, jobs))
     cmd = native_cmd()
     if verbose:
         print(" ".join(cmd), flush=True)

@@ -1,0 +1,4 @@
+// Instantiations of the decode kernel for float message storage.
+#include "relaybp_kernel.cuh"
+
+RBPK_DEFINE_PICK(pick_f32, float)

@@ -1,0 +1,694 @@
+// Device code of the Relay-BP-S decode kernel (sm_100a).  Instantiated per
+// message type by relaybp_inst_*.cu; launched by relaybp.cu (the C ABI).
+//
+// Execution model
+// ---------------
+// A thread block holds `groups` independent groups of `group_threads` (G)
+// threads.  A group decodes one shot at a time, start to finish (first phase,
+// relay legs, selection, outputs), then takes the next shot index from a
+// global atomic work queue: shots that converge early free their group for new
+// work instead of waiting for the slowest shot of a batch.  Groups share only
+// read-only tables; there is no host round trip per iteration.
+//
+// Ownership
+// ---------
+// Thread t of a group owns variables v = t + k*G (k < VPT) and checks
+// c = t + k*G (k < ceil(C/G)).  Everything per variable stays in that thread's
+// registers for the whole kernel: the slot positions of its edges (loaded once
+// per kernel), its posterior (carried across legs: the memory), and the leg's
+// memory strength.  Shared memory per group holds only the edge messages, a
+// per-edge copy of the variable's hard decision, and two bit sets.
+//
+//   msg[rows * C + 1]  edge messages; the slots of check c sit in 16-byte
+//                    chunks (see slot_index), so a check pass moves a row with
+//                    128-bit loads/stores and a warp covers contiguous memory
+//                    (no bank conflicts).  A slot holds mu after a variable pass
+//                    and nu after a check pass.  The last slot is a dummy that
+//                    absent variable edges point at.
+//   hard[rows * C + 1] hard decision of the edge's variable, written by the
+//                    variable pass, read by the next check pass (same index).
+//   best[W], first[W] bit sets (W = ceil(V/32)): best solution, first-leg hard
+//                    decision.
+//
+// Iteration t of a phase (reference: decoder.py:2610-2875):
+//   check pass    (c2v min-sum, kernels.py:1052-1215) + parity of iteration t-1
+//   variable pass (v2c + memory mix + posterior + hard, kernels.py:1220-1350)
+// The parity / selection / freeze of iteration t-1 (kernels.py:510-847) is
+// fused into the check pass of iteration t: each check XORs the hard bytes of
+// its row and a barrier reduction (bar.red.and) tells the whole group whether
+// all checks hold.  The nu such a pass writes after a converged iteration is
+// never read: messages restart at every leg.
+//
+// Numerics follow the reference kernels operation by operation with one
+// rounding per operation (explicit _rn intrinsics; built with --fmad=false);
+// the memory-mix rounding is selectable.  Incoming messages are summed in the
+// graph's var_edges order.  Solution weights are exact 64-bit fixed point.
+
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdint>
+
+#include "relaybp.h"
+
+namespace rbpk {
+
+// ------------------------------------------------------------------ message types
+
+template <typename M>
+struct MsgT;
+template <>
+struct MsgT<float> {
+  using A = float;
+  static __device__ __forceinline__ float ld(float v) { return v; }
+  static __device__ __forceinline__ float st(float v) { return v; }
+};
+template <>
+struct MsgT<double> {
+  using A = double;
+  static __device__ __forceinline__ double ld(double v) { return v; }
+  static __device__ __forceinline__ double st(double v) { return v; }
+};
+template <>
+struct MsgT<__half> {
+  using A = float;
+  static __device__ __forceinline__ float ld(__half v) { return __half2float(v); }
+  static __device__ __forceinline__ __half st(float v) { return __float2half_rn(v); }
+};
+template <>
+struct MsgT<__nv_bfloat16> {
+  using A = float;
+  static __device__ __forceinline__ float ld(__nv_bfloat16 v) { return __bfloat162float(v); }
+  static __device__ __forceinline__ __nv_bfloat16 st(float v) { return __float2bfloat16_rn(v); }
+};
+
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// lambda_mixed = (1 - g) * llr + g * posterior   (kernels.py:1309)
+template <typename A>
+__device__ __forceinline__ A memory_mix(int mode, A g, A l0, A post) {
+  const A one_m = sub_rn(A(1), g);
+  if (mode == RBP_MIX_FMA_GP) return fma_rn(g, post, mul_rn(one_m, l0));
+  if (mode == RBP_MIX_FMA_LP) return fma_rn(one_m, l0, mul_rn(g, post));
+  return add_rn(mul_rn(one_m, l0), mul_rn(g, post));
+}
+
+// Weight of one set bit in units of 2^-32; non-finite priors weigh 0
+// (decoder.py:741-753).  w * 2^32 is exact in float; rounding to nearest-even.
+__device__ __forceinline__ long long weight_units(float w) {
+  if (!isfinite(w)) return 0;
+  return __float2ll_rn(w * 4294967296.0f);
+}
+
+// ------------------------------------------------------------------ group sync
+
+// Barrier over one group: a warp-level sync for 32-thread groups, otherwise a
+// named barrier (id 1 + group index) over the group's threads.
+__device__ __forceinline__ void group_sync(int id, int n) {
+  if (n == 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+  }
+}
+
+// Barrier + AND-reduction of a predicate over the group.
+__device__ __forceinline__ bool group_all(int id, int n, bool p) {
+  if (n == 32) return __all_sync(0xffffffffu, p);
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "bar.red.and.pred po, %2, %3, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)p), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
+// ------------------------------------------------------------------ parameters
+
+struct DevGraph {
+  int C, V, E;
+  int slots;                 // max check degree
+  int rows;                  // slot rows of the layout (padded to MAXDC and to whole 16-byte chunks)
+  int vslots;                // max variable degree (<= MAXDV of the instantiation)
+  const uint8_t* chk_deg;    // [C] (degrees > 255 use the generic check path, which reads chk_ptr)
+  const int* chk_ptr;        // [C+1]
+  const uint16_t* var_pos;   // [vslots, V] slot position of variable v's k-th edge (summation order),
+                             // kNoSlot where v has fewer edges
+};
+
+struct DevArgs {
+  // parameters
+  int pre_iter, num_sets, set_max_iter, stop_nconv;
+  int last_leg, use_alpha, use_beta, mix_mode, skip_legs;
+  float beta, gamma0;
+  // tables
+  const float* llr;              // [V]
+  const long long* wunits;       // [V]
+  const float* gamma_legs;       // [num_sets, V]
+  const float* alpha;            // [n_alpha]
+  // batch inputs
+  long long B;
+  const uint8_t* syn;            // [B, C]
+  const float* llr_shot;         // [B, V] or null
+  const float* gamma_pre;        // [B, V] or null
+  const float* gamma_legs_shot;  // [B, n_shot_legs, V] or null
+  int n_shot_legs;
+  const float* init_post;        // [B, V] or null
+  // outputs
+  uint8_t* errors;
+  uint32_t* errors_packed;
+  float* weights;
+  long long* wfixed;
+  int* found;
+  int* iters;
+  void* last_post;
+  // scheduling
+  int* queue;
+  int group_threads, groups;
+  // shared-memory layout (byte offsets)
+  int off_chk_deg, off_llr, off_group0, group_bytes;
+  int g_msg, g_hard, g_best, g_first, g_red;
+};
+
+enum HardSrc { HARD_ZERO = 0, HARD_POST = 1, HARD_BEST = 2 };
+constexpr uint16_t kNoSlot = 0xFFFFu;
+
+// Shared-memory index of slot j of check c.  The slots of a check are
+// contiguous in 16-byte chunks of VEC = 16 / sizeof(M) messages:
+//   index = (j / VEC) * (VEC * C) + c * VEC + j % VEC
+// so a check pass reads a row with 128-bit loads and consecutive checks are
+// consecutive chunks (a warp covers 512 contiguous bytes per chunk: no bank
+// conflicts).  The per-edge hard bytes use the same index.
+template <typename M>
+__host__ __device__ __forceinline__ int slot_index(int j, int c, int C) {
+  constexpr int VEC = 16 / (int)sizeof(M);
+  return (j / VEC) * (VEC * C) + c * VEC + (j % VEC);
+}
+
+// 16-byte vector access to VEC consecutive slots, converted to/from the
+// accumulation type; hard_word folds the chunk's hard bytes (0/1 each, the
+// first `valid` of them real) into a word whose popcount parity is theirs.
+template <typename M>
+struct VecIO;
+template <>
+struct VecIO<float> {
+  static constexpr int N = 4;
+  static __device__ __forceinline__ void load(const float* p, float* o) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+  }
+  static __device__ __forceinline__ void store(float* p, const float* o) {
+    *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  }
+  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(p);
+    return valid >= 4 ? w : (valid <= 0 ? 0u : w & ((1u << (8 * valid)) - 1u));
+  }
+};
+template <>
+struct VecIO<double> {
+  static constexpr int N = 2;
+  static __device__ __forceinline__ void load(const double* p, double* o) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    o[0] = v.x; o[1] = v.y;
+  }
+  static __device__ __forceinline__ void store(double* p, const double* o) {
+    *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+  }
+  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid) {
+    const uint32_t w = *reinterpret_cast<const uint16_t*>(p);
+    return valid >= 2 ? w : (valid <= 0 ? 0u : w & 0xFFu);
+  }
+};
+template <typename H, float (*ToF)(H), H (*FromF)(float), unsigned short (*Bits)(H), H (*FromBits)(unsigned short)>
+struct VecIO16 {
+  static constexpr int N = 8;
+  static __device__ __forceinline__ void load(const H* p, float* o) {
+    const uint4 v = *reinterpret_cast<const uint4*>(p);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      o[2 * i] = ToF(FromBits((unsigned short)(w[i] & 0xFFFFu)));
+      o[2 * i + 1] = ToF(FromBits((unsigned short)(w[i] >> 16)));
+    }
+  }
+  static __device__ __forceinline__ void store(H* p, const float* o) {
+    uint32_t w[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      w[i] = (uint32_t)Bits(FromF(o[2 * i])) | ((uint32_t)Bits(FromF(o[2 * i + 1])) << 16);
+    *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid) {
+    const uint2 w = *reinterpret_cast<const uint2*>(p);
+    const uint32_t lo = valid >= 4 ? w.x : (valid <= 0 ? 0u : w.x & ((1u << (8 * valid)) - 1u));
+    const int v2 = valid - 4;
+    const uint32_t hi = v2 >= 4 ? w.y : (v2 <= 0 ? 0u : w.y & ((1u << (8 * v2)) - 1u));
+    return lo ^ hi;
+  }
+};
+__device__ __forceinline__ float h2f(__half h) { return __half2float(h); }
+__device__ __forceinline__ __half f2h(float f) { return __float2half_rn(f); }
+__device__ __forceinline__ unsigned short hbits(__half h) { return __half_as_ushort(h); }
+__device__ __forceinline__ __half hfrom(unsigned short b) { return __ushort_as_half(b); }
+__device__ __forceinline__ float b2f(__nv_bfloat16 h) { return __bfloat162float(h); }
+__device__ __forceinline__ __nv_bfloat16 f2b(float f) { return __float2bfloat16_rn(f); }
+__device__ __forceinline__ unsigned short bbits(__nv_bfloat16 h) { return __bfloat16_as_ushort(h); }
+__device__ __forceinline__ __nv_bfloat16 bfrom(unsigned short b) { return __ushort_as_bfloat16(b); }
+template <>
+struct VecIO<__half> : VecIO16<__half, h2f, f2h, hbits, hfrom> {};
+template <>
+struct VecIO<__nv_bfloat16> : VecIO16<__nv_bfloat16, b2f, f2b, bbits, bfrom> {};
+
+// Largest thread block an instantiation with VPT owned variables per thread
+// is compiled for; bounds the registers the owned-variable state may take.
+__host__ __device__ constexpr int max_block_threads(int vpt) {
+  return vpt <= 2 ? 1024 : (vpt == 3 ? 896 : (vpt == 4 ? 768 : (vpt <= 8 ? 512 : 256)));
+}
+
+// Bit set of the hard decisions post <= 0 of the group's variables into dst
+// (one ballot per warp and owned-variable slot).
+template <typename A, int VPT>
+__device__ __forceinline__ void ballot_post(const A (&post)[VPT], uint32_t* dst, int warp, int lane, int G, int V) {
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const int v0 = warp * 32 + k * G;
+    const unsigned m = __ballot_sync(0xffffffffu, v0 + lane < V && post[k] <= A(0));
+    if (lane == 0 && v0 < V) dst[v0 >> 5] = m;
+  }
+}
+
+// ------------------------------------------------------------------ the kernel
+//
+// M     message storage type (float, __half, __nv_bfloat16, double)
+// MAXDC check degree bound held in registers by the check pass (0: generic loop)
+// VPT   variables owned per thread
+// MAXDV variable degree bound (slot positions held in registers)
+template <typename M, int MAXDC, int VPT, int MAXDV>
+__global__ void __launch_bounds__(max_block_threads(VPT))
+relaybp_decode_kernel(DevGraph g, DevArgs a) {
+  using IO = MsgT<M>;
+  using A = typename IO::A;
+  extern __shared__ __align__(16) unsigned char smem[];
+
+  const int C = g.C, V = g.V;
+  uint8_t* s_chk_deg = smem + a.off_chk_deg;
+  float* s_llr = reinterpret_cast<float*>(smem + a.off_llr);
+  for (int i = threadIdx.x; i < C; i += blockDim.x) s_chk_deg[i] = g.chk_deg[i];
+  for (int i = threadIdx.x; i < V; i += blockDim.x) s_llr[i] = a.llr[i];
+
+  const int G = a.group_threads;
+  const int gid = threadIdx.x / G;
+  const int t = threadIdx.x - gid * G;
+  const int lane = threadIdx.x & 31;
+  const int warp = t >> 5;
+  const int nwarps = G >> 5;
+  const int bar = 1 + gid;
+  const int W = (V + 31) >> 5;
+  const int S = a.stop_nconv;
+
+  // slot positions of the owned variables' edges, two 16-bit slots per word;
+  // absent edges (degree < MAXDV) point at the dummy slot after the last row
+  const uint32_t dummy = (uint32_t)(g.rows * C);
+  uint32_t vpos[VPT][(MAXDV + 1) / 2];
+#pragma unroll
+  for (int k = 0; k < VPT; ++k) {
+    const int v = t + k * G;
+#pragma unroll
+    for (int j = 0; j < (MAXDV + 1) / 2; ++j) {
+      uint32_t lo = dummy, hi = dummy;
+      if (v < V) {
+        if (2 * j < g.vslots) lo = g.var_pos[(2 * j) * V + v];
+        if (2 * j + 1 < g.vslots) hi = g.var_pos[(2 * j + 1) * V + v];
+      }
+      lo = lo == kNoSlot ? dummy : lo;
+      hi = hi == kNoSlot ? dummy : hi;
+      vpos[k][j] = lo | (hi << 16);
+    }
+  }
+  __syncthreads();
+  if (gid >= a.groups) return;
+
+  unsigned char* gsm = smem + a.off_group0 + gid * a.group_bytes;
+  M* msg = reinterpret_cast<M*>(gsm + a.g_msg);
+  uint8_t* hard = gsm + a.g_hard;
+  uint32_t* best_bits = reinterpret_cast<uint32_t*>(gsm + a.g_best);
+  uint32_t* first_bits = reinterpret_cast<uint32_t*>(gsm + a.g_first);
+  long long* red = reinterpret_cast<long long*>(gsm + a.g_red);
+  volatile long long* shot_slot = red + nwarps;
+  const A beta = A(a.beta);
+
+  A post[VPT];
+  A gam[VPT];
+
+  while (true) {
+    if (t == 0) *shot_slot = (long long)atomicAdd(a.queue, 1);
+    group_sync(bar, G);
+    const long long b = *shot_slot;
+    if (b >= a.B) break;
+
+    // ---------------- per-shot setup (decoder.py:3429-3478)
+    const uint8_t* syn_row = a.syn + b * (long long)C;
+    uint32_t synm = 0;  // bit k: syndrome of check t + k*G
+    {
+      int k = 0;
+      for (int c = t; c < C; c += G, ++k) synm |= (uint32_t)(syn_row[c] & 1) << k;
+    }
+    const float* llr_row = a.llr_shot ? a.llr_shot + b * (long long)V : nullptr;
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) {
+      const int v = t + k * G;
+      A p0 = A(0);
+      if (v < V) {
+        if (a.init_post) p0 = A(__ldg(a.init_post + b * (long long)V + v));
+        else p0 = llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]);
+      }
+      post[k] = p0;
+    }
+    for (int w = t; w < W; w += G) {
+      best_bits[w] = 0u;
+      first_bits[w] = 0u;
+    }
+    long long best_w = LLONG_MAX;
+    int found = 0, iters = 0, hard_src = HARD_ZERO, sought = 1;
+    bool has_best = false;
+    const int pre = a.pre_iter;
+
+    // Phase -1: the pre-iterations (decoder.py:3480-3616); phase l >= 0: relay
+    // leg l (decoder.py:3672-3837).
+    for (int phase = -1; phase < a.num_sets; ++phase) {
+      int max_iter;
+      const float* grow;
+      float gs = 0.f;
+      if (phase < 0) {
+        max_iter = pre;
+        grow = a.gamma_pre ? a.gamma_pre + b * (long long)V : nullptr;
+        gs = a.gamma0;
+      } else {
+        if (found >= S) break;
+        sought = found + 1;
+        max_iter = a.set_max_iter;
+        grow = (a.gamma_legs_shot && phase < a.n_shot_legs)
+                   ? a.gamma_legs_shot + (b * (long long)a.n_shot_legs + phase) * V
+                   : a.gamma_legs + (long long)phase * V;
+      }
+
+      if (max_iter <= 0) {
+        // freeze_finished_lanes_kernel(count_iteration=False) after an empty phase
+        if (found >= min(sought, S)) hard_src = HARD_BEST;
+      } else {
+        // memory strengths of this phase; message init mu_e = llr[var(e)] (kernels.py:904-1000)
+#pragma unroll
+        for (int k = 0; k < VPT; ++k) {
+          const int v = t + k * G;
+          if (v < V) {
+            gam[k] = grow ? A(__ldg(grow + v)) : A(gs);
+            const M m0 = IO::st(llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]));
+#pragma unroll
+            for (int j = 0; j < MAXDV; ++j) msg[(vpos[k][j >> 1] >> ((j & 1) * 16)) & 0xFFFFu] = m0;
+          }
+        }
+        group_sync(bar, G);
+        int valid = 0;
+        bool frozen = false;
+        for (int it = 0; it <= max_iter; ++it) {
+          const bool check_parity = it > 0;
+          const bool write_nu = it < max_iter;
+          const A alpha = (a.use_alpha && write_nu) ? A(__ldg(a.alpha + it)) : A(1);
+
+          // ---------------- check pass (kernels.py:1052-1215) + parity of it-1 (kernels.py:510-569)
+          bool ok_all = true;
+          int k = 0;
+          for (int c = t; c < C; c += G, ++k) {
+            const int s = (int)((synm >> k) & 1u);
+            int hp = 0, neg = 0, cnt1 = 0;
+            A min1 = A(1e30), min2 = A(1e30);
+            if constexpr (MAXDC > 0) {
+              // The row's slots are contiguous in 16-byte chunks (VEC messages each)
+              // and padded to MAXDC: NQ vector loads/stores, padding masked by selects.
+              constexpr int NQ = MAXDC / VecIO<M>::N;
+              const int deg = s_chk_deg[c];
+              A mv[MAXDC];
+#pragma unroll
+              for (int q = 0; q < NQ; ++q)
+                VecIO<M>::load(msg + slot_index<M>(q * VecIO<M>::N, c, C), mv + q * VecIO<M>::N);
+              if (check_parity) {
+                uint32_t x = 0;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                  x ^= VecIO<M>::hard_word(hard + slot_index<M>(q * VecIO<M>::N, c, C), deg - q * VecIO<M>::N);
+                ok_all = ok_all && ((__popc(x) & 1) == s);
+              }
+              if (write_nu) {
+                // min1 = min(1e30, |mu_j|), min2 = the second smallest (a tie gives
+                // min2 == min1): the argmin edge receives min2 exactly when it is
+                // unique, as in kernels.py:1128-1194.  NaN magnitudes are ignored,
+                // like the reference's comparisons.
+                const A kInf = A(__int_as_float(0x7f800000));
+#pragma unroll
+                for (int j = 0; j < MAXDC; ++j) {
+                  const bool in = j < deg;
+                  neg ^= (in && mv[j] < A(0)) ? 1 : 0;  // parity of negative messages (kernels.py:1134)
+                  const A x = in ? fmin(fabs(mv[j]), kInf) : kInf;
+                  min2 = fmin(min2, fmax(min1, x));
+                  min1 = fmin(min1, x);
+                }
+                const bool par = ((neg ^ s) & 1) != 0;
+                A lo = deg == 1 ? A(0) : min1;
+                A hi = deg == 1 ? A(0) : min2;
+                if (a.use_alpha) {
+                  lo = mul_rn(alpha, lo);
+                  hi = mul_rn(alpha, hi);
+                }
+                if (a.use_beta) {
+                  lo = fmax(sub_rn(lo, beta), A(0));
+                  hi = fmax(sub_rn(hi, beta), A(0));
+                }
+                A out[MAXDC];
+#pragma unroll
+                for (int j = 0; j < MAXDC; ++j) {
+                  const A m = mv[j];
+                  const A mag = (fabs(m) == min1) ? hi : lo;
+                  // sign (mu >= 0 ? 1 : -1) * parity sign (kernels.py:1189-1202)
+                  out[j] = (par != !(m >= A(0))) ? -mag : mag;
+                }
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                  VecIO<M>::store(msg + slot_index<M>(q * VecIO<M>::N, c, C), out + q * VecIO<M>::N);
+              }
+            } else {
+              const int deg = g.chk_ptr[c + 1] - g.chk_ptr[c];
+              for (int j = 0; j < deg; ++j) {
+                const int ix = slot_index<M>(j, c, C);
+                const A m = IO::ld(msg[ix]);
+                if (check_parity) hp ^= hard[ix];
+                neg ^= (m < A(0)) ? 1 : 0;
+                const A x = fabs(m);
+                if (x < min1) { min2 = min1; min1 = x; cnt1 = 1; }
+                else if (x == min1) { cnt1 += 1; }
+                else if (x < min2) { min2 = x; }
+              }
+              if (check_parity) ok_all = ok_all && ((hp & 1) == s);
+              if (write_nu) {
+                const bool par = ((neg ^ s) & 1) != 0;
+                for (int j = 0; j < deg; ++j) {
+                  const int ix = slot_index<M>(j, c, C);
+                  const A m = IO::ld(msg[ix]);
+                  A mag = (cnt1 == 1 && fabs(m) == min1) ? min2 : min1;
+                  if (deg == 1) mag = A(0);
+                  if (a.use_alpha) mag = mul_rn(alpha, mag);
+                  if (a.use_beta) mag = fmax(sub_rn(mag, beta), A(0));
+                  msg[ix] = IO::st((par != !(m >= A(0))) ? -mag : mag);
+                }
+              }
+            }
+          }
+          const bool all_ok = group_all(bar, G, ok_all);
+
+          if (check_parity) {
+            // check_and_select_kernel (kernels.py:609-741) for iteration it-1
+            if (all_ok) {
+              long long w = 0;
+#pragma unroll
+              for (int kk = 0; kk < VPT; ++kk) {
+                const int v = t + kk * G;
+                if (v < V && post[kk] <= A(0))
+                  w += llr_row ? weight_units(__ldg(llr_row + v)) : __ldg(a.wunits + v);
+              }
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+              if (lane == 0) red[warp] = w;
+              group_sync(bar, G);
+              long long tot = 0;
+              for (int i = 0; i < nwarps; ++i) tot += red[i];
+              if (!has_best || tot < best_w) {
+                best_w = tot;
+                has_best = true;
+                ballot_post<A, VPT>(post, best_bits, warp, lane, G, V);
+              }
+              if (valid == 0) found += 1;
+              valid = 1;
+            }
+            // freeze_finished_lanes_kernel (kernels.py:746-847): this iteration counts
+            if (found >= min(sought, S)) {
+              iters += it;
+              hard_src = HARD_BEST;
+              frozen = true;
+              group_sync(bar, G);  // best_bits and red settled before reuse
+              break;
+            }
+          }
+          if (!write_nu) break;
+
+          // ---------------- variable pass (kernels.py:1220-1350)
+#pragma unroll
+          for (int kk = 0; kk < VPT; ++kk) {
+            const int v = t + kk * G;
+            if (v < V) {
+              const A l0 = llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]);
+              const A lm = memory_mix<A>(a.mix_mode, gam[kk], l0, post[kk]);
+              A nv[MAXDV];
+              A sum = A(0);
+#pragma unroll
+              for (int j = 0; j < MAXDV; ++j) {
+                const uint32_t p = (vpos[kk][j >> 1] >> ((j & 1) * 16)) & 0xFFFFu;
+                nv[j] = IO::ld(msg[p]);
+                // absent edges point at the group's dummy slot and are not summed
+                sum = (p != dummy) ? add_rn(sum, nv[j]) : sum;
+              }
+              const A pv = add_rn(lm, sum);
+              post[kk] = pv;
+              const uint8_t h = pv <= A(0) ? 1 : 0;
+#pragma unroll
+              for (int j = 0; j < MAXDV; ++j) {
+                const uint32_t p = (vpos[kk][j >> 1] >> ((j & 1) * 16)) & 0xFFFFu;
+                msg[p] = IO::st(add_rn(lm, sub_rn(sum, nv[j])));
+                hard[p] = h;
+              }
+            }
+          }
+          hard_src = HARD_POST;
+          group_sync(bar, G);
+        }
+        if (!frozen) iters += max_iter;
+      }
+
+      // first-leg hard decision: after the pre-iterations, or after relay leg 1
+      // when there were none (decoder.py:3595-3598, 3807-3810)
+      if (!a.last_leg && (phase < 0 || (phase == 0 && pre == 0))) {
+        group_sync(bar, G);
+        if (hard_src == HARD_POST) {
+          ballot_post<A, VPT>(post, first_bits, warp, lane, G, V);
+        } else {
+          for (int w = t; w < W; w += G) first_bits[w] = hard_src == HARD_BEST ? best_bits[w] : 0u;
+        }
+        group_sync(bar, G);
+      }
+      if (phase < 0 && (found >= S || a.skip_legs)) break;
+    }
+
+    // ---------------- outputs, decoder.py:3839-3873
+    group_sync(bar, G);
+    const uint32_t* src_bits = has_best ? best_bits : first_bits;
+    const bool from_post = !has_best && a.last_leg && hard_src == HARD_POST;
+    const bool zero_bits = !has_best && a.last_leg && hard_src != HARD_POST;
+    if (a.errors) {
+      uint8_t* erow = a.errors + b * (long long)V;
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) {
+        const int v = t + k * G;
+        if (v < V) {
+          uint8_t e;
+          if (from_post) e = post[k] <= A(0) ? 1 : 0;
+          else if (zero_bits) e = 0;
+          else e = (src_bits[v >> 5] >> (v & 31)) & 1u;
+          erow[v] = e;
+        }
+      }
+    }
+    if (a.errors_packed) {
+      uint32_t* prow = a.errors_packed + b * (long long)W;
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) {
+        const int v0 = warp * 32 + k * G;
+        unsigned m;
+        if (from_post) m = __ballot_sync(0xffffffffu, v0 + lane < V && post[k] <= A(0));
+        else if (zero_bits) m = 0u;
+        else m = v0 < V ? src_bits[v0 >> 5] : 0u;
+        if (lane == 0 && v0 < V) prow[v0 >> 5] = m;
+      }
+    }
+    if (a.last_post) {
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) {
+        const int v = t + k * G;
+        if (v < V) {
+          if constexpr (sizeof(A) == 8) reinterpret_cast<double*>(a.last_post)[b * (long long)V + v] = post[k];
+          else reinterpret_cast<float*>(a.last_post)[b * (long long)V + v] = post[k];
+        }
+      }
+    }
+    if (t == 0) {
+      if (a.weights)
+        a.weights[b] = has_best ? __ll2float_rn(best_w) * 2.3283064365386963e-10f  // 2^-32
+                                : __int_as_float(0x7f800000);
+      if (a.wfixed) a.wfixed[b] = has_best ? best_w : LLONG_MAX;
+      a.found[b] = found;
+      a.iters[b] = iters;
+    }
+    group_sync(bar, G);
+  }
+}
+
+using KernelFn = void (*)(DevGraph, DevArgs);
+
+// Kernel for (check degree bound, variable degree, owned variables per thread),
+// or null when this build has no such instantiation.  One per message type.
+KernelFn pick_f32(int dc, int dv, int vpt);
+KernelFn pick_f16(int dc, int dv, int vpt);
+KernelFn pick_bf16(int dc, int dv, int vpt);
+KernelFn pick_f64(int dc, int dv, int vpt);
+
+// Supported owned-variable counts, ascending.
+constexpr int kVptChoices[] = {1, 2, 3, 4, 6, 8, 12, 16};
+
+}  // namespace rbpk
+
+// Instantiation table of one message type (used by relaybp_inst_*.cu).
+#define RBPK_DC_DV(M, DC, VPT)                                                 \
+  if (dv <= 3) return &rbpk::relaybp_decode_kernel<M, DC, VPT, 3>;             \
+  if (dv <= 8) return &rbpk::relaybp_decode_kernel<M, DC, VPT, 8>;             \
+  return nullptr;
+#define RBPK_DC(M, VPT)                                                        \
+  if (dc <= 8) { RBPK_DC_DV(M, 8, VPT) }                                       \
+  if (dc <= 16) { RBPK_DC_DV(M, 16, VPT) }                                     \
+  { RBPK_DC_DV(M, 0, VPT) }
+#define RBPK_DEFINE_PICK(NAME, M)                                              \
+  rbpk::KernelFn rbpk::NAME(int dc, int dv, int vpt) {                         \
+    switch (vpt) {                                                             \
+      case 1: { RBPK_DC(M, 1) }                                                \
+      case 2: { RBPK_DC(M, 2) }                                                \
+      case 3: { RBPK_DC(M, 3) }                                                \
+      case 4: { RBPK_DC(M, 4) }                                                \
+      case 6: { RBPK_DC(M, 6) }                                                \
+      case 8: { RBPK_DC(M, 8) }                                                \
+      case 12: { RBPK_DC(M, 12) }                                              \
+      case 16: { RBPK_DC(M, 16) }                                              \
+      default: return nullptr;                                                 \
+    }                                                                          \
+  }

@@ -67,7 +67,7 @@ def test_graph_create_rejects_malformed_input(case):
 
 
 def test_graph_create_rejects_oversized_layout():
-    """A shot's messages must fit the shared-memory layout (slots * C <= 65535)."""
+    """A shot's messages must fit the shared-memory layout (padded degree * C < 65535)."""
     lib = nat.lib()
     C, deg = 10000, 7
     V = C * deg

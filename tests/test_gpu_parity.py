@@ -231,7 +231,7 @@ def test_full_size_batch_and_permutation_invariance(bb144_full):
         np.testing.assert_array_equal(sub[k], out[k][idx])
 
 
-@pytest.mark.parametrize("shape", [(64, 1), (128, 2), (256, 1), (512, 1)])
+@pytest.mark.parametrize("shape", [(192, 1), (256, 1), (448, 1), (512, 1), (768, 1), (864, 1)])
 def test_launch_shape_invariance(shape):
     w = codes.workload("bb144_phen")
     err, syn = w.sample(512, seed=12)
