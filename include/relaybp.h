@@ -149,6 +149,52 @@ typedef struct {
 RBP_API int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs* out,
                void* stream);
 
+/* Size of the scratch array that rbp_decode_static uses (1 MiB per GPU). */
+#define RBP_STATIC_SCRATCH_BYTES (1 << 20)
+
+/*
+ * Decode B shots without allocating anything.  This entry point has no
+ * counterpart in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc while they decode: a real-time
+ * decoding service with a fixed device-memory budget, which cannot afford the
+ * device-wide synchronisation and unbounded latency of an allocation between
+ * syndrome rounds, or a process whose device memory is already reserved by
+ * another allocator (for example torch's caching allocator), where a new
+ * allocation may fail.
+ *
+ * It takes the whole problem in one call, with no rbp_graph or rbp_decoder:
+ *   - the graph as host arrays, exactly as for rbp_graph_create;
+ *   - the parameters;
+ *   - device pointers to the prior LLRs [V], the leg table [num_sets, V] and
+ *     the alpha table [n_alpha] (may be NULL when use_alpha == 0);
+ *   - the batch inputs and outputs, as for rbp_decode.
+ * It decodes with the same kernel as rbp_decode, so the results are identical.
+ *
+ * The graph tables it derives (check degrees, check pointers, slot positions)
+ * and the kernel's work-queue counter live in a static device array of
+ * RBP_STATIC_SCRATCH_BYTES bytes.  That array is part of the library image:
+ * every GPU that loads the library holds it until the process exits.  A graph
+ * whose tables need more returns RBP_ERR_UNSUPPORTED.  The call neither
+ * allocates nor frees memory, on the device or on the host; it stages the
+ * tables through a fixed stack buffer.
+ *
+ * All calls share that one array, and each call overwrites it: the counter is
+ * cleared and every table is rewritten.  Calls that overlap on the GPU (on
+ * different streams, or from different host threads) therefore race and give
+ * wrong results; serialise them on one stream.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it.  Make that first call before any
+ * stream capture begins.
+ */
+RBP_API int rbp_decode_static(int32_t C, int32_t V, int32_t E,
+                              const int32_t* chk_ptr, const int32_t* edge_var,
+                              const int32_t* var_ptr, const int32_t* var_edges,
+                              const rbp_params* p, const float* llr, const float* gamma_legs,
+                              const float* alpha, int32_t n_alpha, int32_t device,
+                              int64_t B, const rbp_batch* in, const rbp_outputs* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

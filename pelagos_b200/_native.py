@@ -40,7 +40,11 @@ EXPORTED_SYMBOLS = (
     "rbp_decoder_configure",
     "rbp_decoder_query",
     "rbp_decode",
+    "rbp_decode_static",
 )
+
+#: Bytes of the static scratch array rbp_decode_static uses (RBP_STATIC_SCRATCH_BYTES).
+STATIC_SCRATCH_BYTES = 1 << 20
 
 
 class NativeLibraryError(RuntimeError):
@@ -116,6 +120,9 @@ def _declare(lib):
     lib.rbp_decoder_query.argtypes = [P, ct.POINTER(i64), ct.POINTER(i64), i32p, i32p, i32p]
     lib.rbp_decode.restype = ct.c_int
     lib.rbp_decode.argtypes = [P, i64, ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs), P]
+    lib.rbp_decode_static.restype = ct.c_int
+    lib.rbp_decode_static.argtypes = [i32, i32, i32, i32p, i32p, i32p, i32p, ct.POINTER(RbpParams), P, P, P, i32,
+                                      i32, i64, ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs), P]
     return lib
 
 

@@ -128,16 +128,16 @@ int slot_index_host(int j, int c, int C, int msg_type) {
 }
 
 // Block-wide tables first, then one region per group.
-Layout make_layout(const rbp_graph* g, int rows, int msg_type, int group_threads) {
+Layout make_layout(int C, int V, int rows, int msg_type, int group_threads) {
   Layout L{};
   int o = 0;
   L.off_chk_deg = o;
-  o = align16(o + g->C);
+  o = align16(o + C);
   L.off_llr = o;
-  o = align16(o + 4 * g->V);
+  o = align16(o + 4 * V);
   L.off_group0 = o;
-  const int slots_total = rows * g->C + 1;  // + the dummy slot of absent variable edges
-  const int W = (g->V + 31) / 32;
+  const int slots_total = rows * C + 1;  // + the dummy slot of absent variable edges
+  const int W = (V + 31) / 32;
   int q = 0;
   L.g_msg = q;
   q = align16(q + (int)msg_size(msg_type) * slots_total);
@@ -173,10 +173,145 @@ int vpt_for(int V, int G) {
 
 // Default shape: the fewest threads per shot with at most 3 variables each
 // (rounded to whole warps, at most 1024), so a shot's iteration is short.
-int default_group_threads(const rbp_graph* g) {
-  int G = ((g->V + 2) / 3 + 31) / 32 * 32;
-  G = std::max(G, ((g->C + 31) / 32 + 31) / 32 * 32);
+int default_group_threads(int C, int V) {
+  int G = ((V + 2) / 3 + 31) / 32 * 32;
+  G = std::max(G, ((C + 31) / 32 + 31) / 32 * 32);
   return std::min(std::max(G, 32), 1024);
+}
+
+struct Launch {
+  KernelFn kernel;
+  int group_threads, groups, blocks;
+};
+
+// Kernel and launch shape for G threads per group (groups_per_block 0: as many as fit).
+int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int groups_per_block,
+                  size_t max_smem, int sm_count, Launch* out, const char* who) {
+  const std::string w(who);
+  if (G % 32 != 0 || G > 1024)
+    return fail(RBP_ERR_ARGUMENT, w + ": group_threads must be a multiple of 32, at most 1024");
+  const int vpt = vpt_for(V, G);
+  if (vpt < 0) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 16 variables per thread; use more group threads");
+  if ((C + G - 1) / G > 32) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 32 checks per thread; use more group threads");
+  const int max_threads = rbpk::max_block_threads(vpt);
+  if (G > max_threads)
+    return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +
+                                         " variables each exceed the register budget");
+  KernelFn k = pick_kernel(msg_type, slots, vslots, vpt);
+  if (!k) return fail(RBP_ERR_UNSUPPORTED, w + ": no kernel for this degree / shape");
+  const Layout L = make_layout(C, V, rows, msg_type, G);
+  const size_t block_fixed = (size_t)L.off_group0;
+  if (block_fixed + L.group_bytes > max_smem)
+    return fail(RBP_ERR_UNSUPPORTED,
+                w + ": one shot's state (" + std::to_string(L.group_bytes) + " B) does not fit in shared memory");
+  int max_groups = (int)((max_smem - block_fixed) / L.group_bytes);
+  max_groups = std::min(max_groups, max_threads / G);
+  if (G != 32) max_groups = std::min(max_groups, 15);  // named barriers 1..15
+  const int NG = groups_per_block > 0 ? groups_per_block : max_groups;
+  if (NG < 1 || NG > max_groups)
+    return fail(RBP_ERR_UNSUPPORTED,
+                w + ": groups_per_block must be in [1, " + std::to_string(max_groups) + "] for this shape");
+  // The attribute is per kernel function and shared by every decoder that uses
+  // this instantiation, so it is set to the device limit; occupancy uses `smem`.
+  RBP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+  const size_t smem = block_fixed + (size_t)NG * L.group_bytes;
+  int per_sm = 0;
+  RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * NG, smem));
+  if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
+  *out = Launch{k, G, NG, per_sm * sm_count};
+  return RBP_OK;
+}
+
+int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outputs* out, const rbp_params& p,
+                int n_alpha) {
+  const std::string w(who);
+  if (B < 0) return fail(RBP_ERR_ARGUMENT, w + ": negative batch");
+  if (B > INT_MAX) return fail(RBP_ERR_UNSUPPORTED, w + ": batch exceeds 2^31-1 shots");
+  if (B == 0) return RBP_OK;
+  if (!in->syndromes || !out->found_count || !out->iterations)
+    return fail(RBP_ERR_ARGUMENT, w + ": syndromes, found_count and iterations are required");
+  if (in->pre_iter < 0) return fail(RBP_ERR_ARGUMENT, w + ": pre_iter must be >= 0");
+  if (p.use_alpha && in->pre_iter > n_alpha) return fail(RBP_ERR_ARGUMENT, w + ": pre_iter exceeds the alpha table");
+  if (in->n_shot_legs < 0 || (in->n_shot_legs > 0 && !in->gamma_legs_shot))
+    return fail(RBP_ERR_ARGUMENT, w + ": gamma_legs_shot missing");
+  return RBP_OK;
+}
+
+// Fill the kernel arguments and launch (memset of the work counter + kernel) on `st`.
+int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, const Launch& lc, const float* llr,
+                  const long long* wunits, const float* gamma_legs, const float* alpha, int* queue, int64_t B,
+                  const rbp_batch* in, const rbp_outputs* out, cudaStream_t st, const char* who) {
+  DevArgs a{};
+  a.pre_iter = in->pre_iter;
+  a.num_sets = p.num_sets;
+  a.set_max_iter = p.set_max_iter;
+  a.stop_nconv = p.stop_nconv;
+  a.last_leg = p.last_leg;
+  a.use_alpha = p.use_alpha;
+  a.use_beta = p.use_beta;
+  a.mix_mode = p.mix_mode;
+  a.skip_legs = in->skip_relay_legs;
+  a.beta = p.beta;
+  a.gamma0 = in->gamma0;
+  a.llr = llr;
+  a.wunits = wunits;
+  a.gamma_legs = gamma_legs;
+  a.alpha = alpha;
+  a.B = B;
+  a.syn = in->syndromes;
+  a.llr_shot = in->llr_per_shot;
+  a.gamma_pre = in->gamma_pre;
+  a.gamma_legs_shot = in->gamma_legs_shot;
+  a.n_shot_legs = in->n_shot_legs;
+  a.init_post = in->init_posterior;
+  a.errors = out->errors;
+  a.errors_packed = out->errors_packed;
+  a.weights = out->weights;
+  a.wfixed = reinterpret_cast<long long*>(out->weight_fixed);
+  a.found = out->found_count;
+  a.iters = out->iterations;
+  a.last_post = out->last_posterior;
+  a.queue = queue;
+  a.group_threads = lc.group_threads;
+  a.groups = lc.groups;
+  a.off_chk_deg = L.off_chk_deg;
+  a.off_llr = L.off_llr;
+  a.off_group0 = L.off_group0;
+  a.group_bytes = L.group_bytes;
+  a.g_msg = L.g_msg;
+  a.g_hard = L.g_hard;
+  a.g_best = L.g_best;
+  a.g_first = L.g_first;
+  a.g_red = L.g_red;
+  const long long need_blocks = (B + lc.groups - 1) / lc.groups;
+  const int blocks = (int)std::min<long long>(lc.blocks, need_blocks);
+  const size_t smem = (size_t)L.off_group0 + (size_t)lc.groups * L.group_bytes;
+  cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), st);
+  if (e != cudaSuccess) return fail(RBP_ERR_CUDA, std::string(who) + ": cudaMemsetAsync: " + cudaGetErrorString(e));
+  lc.kernel<<<blocks, lc.group_threads * lc.groups, smem, st>>>(dgph, a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(RBP_ERR_CUDA, std::string(who) + ": launch: " + cudaGetErrorString(e));
+  return RBP_OK;
+}
+
+// Scratch of rbp_decode_static: the work counter and the graph tables of the
+// current call.  Every device that loads the library holds it until exit.
+static __device__ __align__(256) unsigned char g_static_scratch[RBP_STATIC_SCRATCH_BYTES];
+
+// Device address of g_static_scratch on `device` (the current device), looked
+// up on the first call per device and cached.
+int static_scratch(int device, unsigned char** out) {
+  static void* cached[64] = {};
+  if (device < 0 || device >= 64) return fail(RBP_ERR_UNSUPPORTED, "rbp_decode_static: device ordinal above 63");
+  if (!cached[device]) {
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess)
+      return fail(RBP_ERR_CUDA, std::string("rbp_decode_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    cached[device] = ptr;
+  }
+  *out = static_cast<unsigned char*>(cached[device]);
+  return RBP_OK;
 }
 
 }  // namespace
@@ -262,47 +397,20 @@ int rbp_graph_destroy(rbp_graph* g) {
 int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: null decoder");
   const rbp_graph* g = d->g;
-  const int G = group_threads > 0 ? group_threads : default_group_threads(g);
-  if (G % 32 != 0 || G > 1024)
-    return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: group_threads must be a multiple of 32, at most 1024");
-  const int vpt = vpt_for(g->V, G);
-  if (vpt < 0)
-    return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: more than 16 variables per thread; use more group threads");
-  if ((g->C + G - 1) / G > 32)
-    return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: more than 32 checks per thread; use more group threads");
-  const int max_threads = rbpk::max_block_threads(vpt);
-  if (G > max_threads)
-    return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: " + std::to_string(G) + " threads with " +
-                                         std::to_string(vpt) + " variables each exceed the register budget");
-  KernelFn k = pick_kernel(d->p.msg_type, g->slots, g->vslots, vpt);
-  if (!k) return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: no kernel for this degree / shape");
-  const Layout L = make_layout(g, d->rows, d->p.msg_type, G);
-  const size_t block_fixed = (size_t)L.off_group0;
-  if (block_fixed + L.group_bytes > d->max_smem)
-    return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: one shot's state (" + std::to_string(L.group_bytes) +
-                                         " B) does not fit in shared memory");
-  int max_groups = (int)((d->max_smem - block_fixed) / L.group_bytes);
-  max_groups = std::min(max_groups, max_threads / G);
-  if (G != 32) max_groups = std::min(max_groups, 15);  // named barriers 1..15
-  const int NG = groups_per_block > 0 ? groups_per_block : max_groups;
-  if (NG < 1 || NG > max_groups)
-    return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: groups_per_block must be in [1, " +
-                                         std::to_string(max_groups) + "] for this shape");
+  const int G = group_threads > 0 ? group_threads : default_group_threads(g->C, g->V);
   DeviceGuard dg(g->device);
-  // The attribute is per kernel function and shared by every decoder that uses
-  // this instantiation, so it is set to the device limit; occupancy uses `smem`.
-  RBP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d->max_smem));
-  const size_t smem = block_fixed + (size_t)NG * L.group_bytes;
-  int per_sm = 0;
-  RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * NG, smem));
-  if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, "rbp_decoder_configure: launch shape has zero occupancy");
-  d->kernel = k;
-  d->vpt = vpt;
-  d->group_threads = G;
-  d->groups = NG;
-  d->blocks = per_sm * d->sm_count;
+  Launch lc{};
+  const int rc = choose_launch(g->C, g->V, g->slots, g->vslots, d->rows, d->p.msg_type, G, groups_per_block,
+                               d->max_smem, d->sm_count, &lc, "rbp_decoder_configure");
+  if (rc != RBP_OK) return rc;
+  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, G);
+  d->kernel = lc.kernel;
+  d->vpt = vpt_for(g->V, G);
+  d->group_threads = lc.group_threads;
+  d->groups = lc.groups;
+  d->blocks = lc.blocks;
   d->group_bytes = L.group_bytes;
-  d->block_bytes = (int)block_fixed;
+  d->block_bytes = L.off_group0;
   return RBP_OK;
 }
 
@@ -398,73 +506,114 @@ int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_
 
 int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs* out, void* stream) {
   if (!d || !in || !out) return fail(RBP_ERR_ARGUMENT, "rbp_decode: null argument");
-  if (B < 0) return fail(RBP_ERR_ARGUMENT, "rbp_decode: negative batch");
-  if (B == 0) return RBP_OK;
-  if (B > INT_MAX) return fail(RBP_ERR_UNSUPPORTED, "rbp_decode: batch exceeds 2^31-1 shots");
-  if (!in->syndromes || !out->found_count || !out->iterations)
-    return fail(RBP_ERR_ARGUMENT, "rbp_decode: syndromes, found_count and iterations are required");
-  if (in->pre_iter < 0) return fail(RBP_ERR_ARGUMENT, "rbp_decode: pre_iter must be >= 0");
-  if (d->p.use_alpha && in->pre_iter > d->n_alpha)
-    return fail(RBP_ERR_ARGUMENT, "rbp_decode: pre_iter exceeds the alpha table");
-  if (in->n_shot_legs < 0 || (in->n_shot_legs > 0 && !in->gamma_legs_shot))
-    return fail(RBP_ERR_ARGUMENT, "rbp_decode: gamma_legs_shot missing");
+  int rc = check_batch("rbp_decode", B, in, out, d->p, d->n_alpha);
+  if (rc != RBP_OK || B == 0) return rc;
   const rbp_graph* g = d->g;
   DeviceGuard dg(g->device);
   if (!dg.ok) return fail(RBP_ERR_CUDA, "rbp_decode: cannot select the CUDA device");
+  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, d->group_threads);
+  const DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
+  const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks};
+  return launch_decode(dgph, d->p, L, lc, d->llr.p, d->wunits.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
+                       out, reinterpret_cast<cudaStream_t>(stream), "rbp_decode");
+}
+
+// ------------------------------------------------------------------ decode without allocation
+
+int rbp_decode_static(int32_t C, int32_t V, int32_t E, const int32_t* chk_ptr, const int32_t* edge_var,
+                      const int32_t* var_ptr, const int32_t* var_edges, const rbp_params* p, const float* llr,
+                      const float* gamma_legs, const float* alpha, int32_t n_alpha, int32_t device, int64_t B,
+                      const rbp_batch* in, const rbp_outputs* out, void* stream) {
+  const char* who = "rbp_decode_static";
+  if (!p || !in || !out || !llr) return fail(RBP_ERR_ARGUMENT, std::string(who) + ": null argument");
+  if (C <= 0 || V <= 0 || E <= 0) return fail(RBP_ERR_ARGUMENT, std::string(who) + ": C, V and E must be positive");
+  if (!chk_ptr || !edge_var || !var_ptr || !var_edges)
+    return fail(RBP_ERR_ARGUMENT, std::string(who) + ": null graph array");
+  if (chk_ptr[0] != 0 || chk_ptr[C] != E || var_ptr[0] != 0 || var_ptr[V] != E)
+    return fail(RBP_ERR_ARGUMENT, std::string(who) + ": chk_ptr/var_ptr must start at 0 and end at E");
+  if (p->msg_type < RBP_MSG_F32 || p->msg_type > RBP_MSG_F64 || p->mix_mode < RBP_MIX_SEPARATE ||
+      p->mix_mode > RBP_MIX_FMA_LP || p->pre_iter < 0 || p->num_sets < 0 || p->set_max_iter < 0)
+    return fail(RBP_ERR_ARGUMENT, std::string(who) + ": invalid parameters");
+  if (p->num_sets > 0 && !gamma_legs) return fail(RBP_ERR_ARGUMENT, std::string(who) + ": gamma_legs is null");
+  if (p->use_alpha && (!alpha || n_alpha < std::max(p->pre_iter, p->set_max_iter)))
+    return fail(RBP_ERR_ARGUMENT, std::string(who) + ": alpha table shorter than max(pre_iter, set_max_iter)");
+  // degrees (no host storage)
+  int slots = 0, vslots = 0;
+  for (int c = 0; c < C; ++c) {
+    if (chk_ptr[c + 1] < chk_ptr[c]) return fail(RBP_ERR_ARGUMENT, std::string(who) + ": chk_ptr not monotone");
+    slots = std::max(slots, chk_ptr[c + 1] - chk_ptr[c]);
+  }
+  for (int v = 0; v < V; ++v) {
+    if (var_ptr[v + 1] < var_ptr[v]) return fail(RBP_ERR_ARGUMENT, std::string(who) + ": var_ptr not monotone");
+    vslots = std::max(vslots, var_ptr[v + 1] - var_ptr[v]);
+  }
+  if (vslots > 8) return fail(RBP_ERR_UNSUPPORTED, std::string(who) + ": variable degree exceeds 8");
+  const int rows = layout_rows(slots, p->msg_type);
+  if ((long long)rows * C >= 65535)
+    return fail(RBP_ERR_UNSUPPORTED, std::string(who) + ": message layout exceeds 65535 slots");
+  // scratch layout: [counter | chk_deg u8 | chk_ptr i32 | var_pos u16]
+  const size_t off_deg = 256;
+  const size_t off_ptr = (off_deg + (size_t)C + 15) / 16 * 16;
+  const size_t off_pos = (off_ptr + 4 * ((size_t)C + 1) + 15) / 16 * 16;
+  const size_t need = off_pos + 2 * (size_t)vslots * V;
+  if (need > (size_t)RBP_STATIC_SCRATCH_BYTES)
+    return fail(RBP_ERR_UNSUPPORTED, std::string(who) + ": graph tables need " + std::to_string(need) +
+                                         " bytes of scratch; the static scratch holds " +
+                                         std::to_string((long long)RBP_STATIC_SCRATCH_BYTES));
+  const int rc0 = check_batch(who, B, in, out, *p, p->use_alpha ? n_alpha : 1);
+  if (rc0 != RBP_OK || B == 0) return rc0;
+  DeviceGuard dg(device);
+  if (!dg.ok) return fail(RBP_ERR_CUDA, std::string(who) + ": cannot select the CUDA device");
+  unsigned char* scratch = nullptr;
+  int rc = static_scratch(device, &scratch);
+  if (rc != RBP_OK) return rc;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const Layout L = make_layout(g, d->rows, d->p.msg_type, d->group_threads);
 
-  DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
-  DevArgs a{};
-  a.pre_iter = in->pre_iter;
-  a.num_sets = d->p.num_sets;
-  a.set_max_iter = d->p.set_max_iter;
-  a.stop_nconv = d->p.stop_nconv;
-  a.last_leg = d->p.last_leg;
-  a.use_alpha = d->p.use_alpha;
-  a.use_beta = d->p.use_beta;
-  a.mix_mode = d->p.mix_mode;
-  a.skip_legs = in->skip_relay_legs;
-  a.beta = d->p.beta;
-  a.gamma0 = in->gamma0;
-  a.llr = d->llr.p;
-  a.wunits = d->wunits.p;
-  a.gamma_legs = d->gamma_legs.p;
-  a.alpha = d->alpha.p;
-  a.B = B;
-  a.syn = in->syndromes;
-  a.llr_shot = in->llr_per_shot;
-  a.gamma_pre = in->gamma_pre;
-  a.gamma_legs_shot = in->gamma_legs_shot;
-  a.n_shot_legs = in->n_shot_legs;
-  a.init_post = in->init_posterior;
-  a.errors = out->errors;
-  a.errors_packed = out->errors_packed;
-  a.weights = out->weights;
-  a.wfixed = reinterpret_cast<long long*>(out->weight_fixed);
-  a.found = out->found_count;
-  a.iters = out->iterations;
-  a.last_post = out->last_posterior;
-  a.queue = d->queue.p;
-  a.group_threads = d->group_threads;
-  a.groups = d->groups;
-  a.off_chk_deg = L.off_chk_deg;
-  a.off_llr = L.off_llr;
-  a.off_group0 = L.off_group0;
-  a.group_bytes = L.group_bytes;
-  a.g_msg = L.g_msg;
-  a.g_hard = L.g_hard;
-  a.g_best = L.g_best;
-  a.g_first = L.g_first;
-  a.g_red = L.g_red;
+  // Tables are staged through a fixed stack buffer; a pageable-memory copy has
+  // consumed the buffer when cudaMemcpyAsync returns, so the buffer is reused.
+  unsigned char stage[4096];
+  size_t fill = 0, at = off_deg;
+  auto flush = [&]() -> int {
+    if (fill) RBP_CUDA(cudaMemcpyAsync(scratch + at, stage, fill, cudaMemcpyHostToDevice, st));
+    at += fill;
+    fill = 0;
+    return RBP_OK;
+  };
+  for (int c = 0; c < C; ++c) {
+    stage[fill++] = (unsigned char)std::min(255, chk_ptr[c + 1] - chk_ptr[c]);
+    if (fill == sizeof(stage) && (rc = flush())) return rc;
+  }
+  if ((rc = flush())) return rc;
+  RBP_CUDA(cudaMemcpyAsync(scratch + off_ptr, chk_ptr, 4 * ((size_t)C + 1), cudaMemcpyHostToDevice, st));
+  at = off_pos;
+  for (int k = 0; k < vslots; ++k) {
+    for (int v = 0; v < V; ++v) {
+      uint16_t pos = rbpk::kNoSlot;
+      const int q = var_ptr[v] + k;
+      if (q < var_ptr[v + 1]) {
+        const int e = var_edges[q];
+        if (e < 0 || e >= E || edge_var[e] != v)
+          return fail(RBP_ERR_ARGUMENT, std::string(who) + ": var_edges is not the variable-major order of edge_var");
+        const int c = (int)(std::upper_bound(chk_ptr, chk_ptr + C + 1, e) - chk_ptr) - 1;  // check of edge e
+        pos = (uint16_t)slot_index_host(e - chk_ptr[c], c, C, p->msg_type);
+      }
+      std::memcpy(stage + fill, &pos, 2);
+      fill += 2;
+      if (fill == sizeof(stage) && (rc = flush())) return rc;
+    }
+  }
+  if ((rc = flush())) return rc;
 
-  const long long need_blocks = (B + d->groups - 1) / d->groups;
-  const int blocks = (int)std::min<long long>(d->blocks, need_blocks);
-  const size_t smem = (size_t)L.off_group0 + (size_t)d->groups * L.group_bytes;
-  RBP_CUDA(cudaMemsetAsync(d->queue.p, 0, sizeof(int), st));
-  d->kernel<<<blocks, d->group_threads * d->groups, smem, st>>>(dgph, a);
-  RBP_CUDA(cudaGetLastError());
-  return RBP_OK;
+  int G = default_group_threads(C, V), max_smem = 0, sms = 0;
+  RBP_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+  RBP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  Launch lc{};
+  if ((rc = choose_launch(C, V, slots, vslots, rows, p->msg_type, G, 0, (size_t)max_smem, sms, &lc, who))) return rc;
+  const Layout L = make_layout(C, V, rows, p->msg_type, G);
+  const DevGraph dgph{C, V, E, slots, rows, vslots, scratch + off_deg, reinterpret_cast<const int*>(scratch + off_ptr),
+                      reinterpret_cast<const uint16_t*>(scratch + off_pos)};
+  return launch_decode(dgph, *p, L, lc, llr, nullptr, gamma_legs, alpha, reinterpret_cast<int*>(scratch), B, in, out,
+                       st, who);
 }
 
 }  // extern "C"

@@ -158,7 +158,7 @@ struct DevArgs {
   float beta, gamma0;
   // tables
   const float* llr;              // [V]
-  const long long* wunits;       // [V]
+  const long long* wunits;       // [V], or null: units computed from llr
   const float* gamma_legs;       // [num_sets, V]
   const float* alpha;            // [n_alpha]
   // batch inputs
@@ -528,7 +528,8 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
               for (int kk = 0; kk < VPT; ++kk) {
                 const int v = t + kk * G;
                 if (v < V && post[kk] <= A(0))
-                  w += llr_row ? weight_units(__ldg(llr_row + v)) : __ldg(a.wunits + v);
+                  w += llr_row ? weight_units(__ldg(llr_row + v))
+                               : (a.wunits ? __ldg(a.wunits + v) : weight_units(s_llr[v]));
               }
 #pragma unroll
               for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
