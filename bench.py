@@ -182,9 +182,15 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shots", type=int, default=SHOTS)
+    ap.add_argument("--launch", default=None, help="G,groups: kernel shape (default: autotuned)")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--workload", default="bb144_phen", choices=["bb144_phen", "mixed"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload == "mixed":
+        run_mixed(args)
         return
 
     import torch
@@ -206,9 +212,14 @@ def main():
     w = codes.workload(WORKLOAD, p=P)
     shots = args.shots
     err, syn = w.sample(shots, seed=SEED + rank)
-    dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], **RELAY)
+    launch = tuple(int(x) for x in args.launch.split(",")) if args.launch else None
+    dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], launch=launch, **RELAY)
     syn_dev = torch.from_numpy(syn).to(dev)
     syn_pin = torch.from_numpy(syn).pin_memory()
+    if launch is None and not args.no_autotune:
+        from pelagos_b200 import autotune
+
+        autotune.tune(dec, syn_dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream()
 
@@ -330,6 +341,71 @@ def main():
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+MIXED = [("bb72_cc", 0.03), ("bb144_cc", 0.03), ("bb144_phen", 0.003), ("ldpc2000", 0.02)]
+
+
+def run_mixed(args) -> None:
+    """262,144 shots split evenly over four codes, decoded by one persistent launch (CUDA-graph replay)
+    versus the four batches decoded one after another by their own decoders."""
+    import torch
+
+    from pelagos_b200 import RelayBPDecoder, codes
+    from pelagos_b200.mixed import MixedDecoder
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    per = 262144 // len(MIXED)
+    decs, syns, ws, errs = [], [], [], []
+    for i, (name, p) in enumerate(MIXED):
+        w = codes.workload(name, p=p)
+        err, syn = w.sample(per, seed=SEED + 10 * i + rank)
+        decs.append(RelayBPDecoder(w.H, w.priors, device=[local], **RELAY))
+        syns.append(torch.from_numpy(syn).to(dev))
+        ws.append(w)
+        errs.append(err)
+    mix = MixedDecoder(decs, graph=True)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        mix.decode(syns)
+        for d, s in zip(decs, syns):
+            d.decode(s)
+    torch.cuda.synchronize()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, out
+
+    ms_mix, outs = timed(lambda: mix.decode(syns))
+    ms_seq, _ = timed(lambda: [d.decode(s) for d, s in zip(decs, syns)])
+    per_code = []
+    for (name, p), w, err, o in zip(MIXED, ws, errs, outs):
+        o = {k: v.cpu().numpy() for k, v in o.items()}
+        conv = o["found_count"] > 0
+        fails = w.logical_failures(err, o["errors"], conv) if w.logicals.shape[0] else \
+            (~conv | np.any(o["errors"] != err, axis=1))
+        per_code.append({"code": name, "p": p, "shots": per, "ler": float(fails.mean()),
+                         "unconverged": int((~conv).sum()), "mean_iterations": float(o["iterations"].mean())})
+    line = {
+        "metric": "shots/s, mixed-code batch in one persistent launch", "value": 262144 / (ms_mix / 1000.0),
+        "unit": "shots/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mix,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded i.i.d. Bernoulli errors, s = H e mod 2)",
+        "config": {"workload": "262,144 shots: [[72,12,6]] cc p=0.03, [[144,12,12]] cc p=0.03, "
+                               "[[144,12,12]] phenomenological p=0.003, (3,6)-regular 2000x4000 p=0.02",
+                   "launch": mix.launch_info()},
+        "separate_launches": {"ms_per_step": ms_seq, "shots_per_s": 262144 / (ms_seq / 1000.0)},
+        "per_code": per_code, "gpu_launches": args.steps,
+    }
+    print(json.dumps(line), flush=True)
 
 
 def _wilson(k: int, n: int, z: float = 1.959964) -> tuple[float, float]:

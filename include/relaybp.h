@@ -149,6 +149,38 @@ typedef struct {
 RBP_API int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs* out,
                void* stream);
 
+/*
+ * Mixed-code launch: several decoders' batches in ONE persistent launch.
+ * Each thread block serves one code at a time, with that code's group shape,
+ * and takes shots from that code's work queue; when the queue is empty the
+ * block moves to the next code that still has shots.  Shots of small and large
+ * codes therefore share the GPU without a launch per code, and converged shots
+ * free their group for any code's remaining work.  Extends the reference's
+ * per-decoder, per-batch-size decode (src/pelagos/decoder.py:1480-1538) and the
+ * host-side "difficult batch" re-queue of pelagos_benchmark.py:1462-1520.
+ * Up to 8 decoders, all on one device, float32 messages.
+ */
+typedef struct rbp_mixed rbp_mixed;
+
+RBP_API int rbp_mixed_create(const rbp_decoder* const* decoders, int32_t n, rbp_mixed** out);
+RBP_API int rbp_mixed_destroy(rbp_mixed* m);
+
+/* Decode batch i (B[i] shots, ins[i], outs[i]) with decoders[i], for all i,
+ * in one launch on `stream` (asynchronous). */
+RBP_API int rbp_mixed_decode(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_outputs* outs,
+                             void* stream);
+
+/* Record the same decode (same sizes and buffers) as a CUDA graph (the queue
+ * reset and the persistent launch); rbp_mixed_replay launches that graph on
+ * `stream`.  A replay reads the captured input buffers and writes the captured
+ * output buffers, so callers refill the inputs in place between replays. */
+RBP_API int rbp_mixed_capture(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_outputs* outs);
+RBP_API int rbp_mixed_replay(rbp_mixed* m, void* stream);
+
+/* Launch shape of code i inside the mixed launch. */
+RBP_API int rbp_mixed_query(const rbp_mixed* m, int32_t i, int32_t* group_threads, int32_t* groups_per_block,
+                            int32_t* block_threads, int32_t* blocks);
+
 /* Size of the scratch array that rbp_decode_static uses (1 MiB per GPU). */
 #define RBP_STATIC_SCRATCH_BYTES (1 << 20)
 

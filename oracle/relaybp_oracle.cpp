@@ -104,7 +104,8 @@ template <> struct Msg<double> {
 };
 template <> struct Msg<half_t> {
   static float load(half_t v) { return f16_to_f32(v.bits); }
-  static half_t store(float v) { return half_t{f32_to_f16(v)}; }
+  // saturate at +-65504 (the largest finite binary16) before rounding, as the kernel does
+  static half_t store(float v) { return half_t{f32_to_f16(std::fmin(std::fmax(v, -65504.0f), 65504.0f))}; }
 };
 template <> struct Msg<bf16_t> {
   static float load(bf16_t v) { return bf16_to_f32(v.bits); }

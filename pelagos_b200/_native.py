@@ -41,6 +41,12 @@ EXPORTED_SYMBOLS = (
     "rbp_decoder_query",
     "rbp_decode",
     "rbp_decode_static",
+    "rbp_mixed_create",
+    "rbp_mixed_destroy",
+    "rbp_mixed_decode",
+    "rbp_mixed_capture",
+    "rbp_mixed_replay",
+    "rbp_mixed_query",
 )
 
 #: Bytes of the static scratch array rbp_decode_static uses (RBP_STATIC_SCRATCH_BYTES).
@@ -123,6 +129,19 @@ def _declare(lib):
     lib.rbp_decode_static.restype = ct.c_int
     lib.rbp_decode_static.argtypes = [i32, i32, i32, i32p, i32p, i32p, i32p, ct.POINTER(RbpParams), P, P, P, i32,
                                       i32, i64, ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs), P]
+    lib.rbp_mixed_create.restype = ct.c_int
+    lib.rbp_mixed_create.argtypes = [ct.POINTER(P), i32, ct.POINTER(P)]
+    lib.rbp_mixed_destroy.restype = ct.c_int
+    lib.rbp_mixed_destroy.argtypes = [P]
+    for f in (lib.rbp_mixed_decode,):
+        f.restype = ct.c_int
+        f.argtypes = [P, ct.POINTER(i64), ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs), P]
+    lib.rbp_mixed_capture.restype = ct.c_int
+    lib.rbp_mixed_capture.argtypes = [P, ct.POINTER(i64), ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs)]
+    lib.rbp_mixed_replay.restype = ct.c_int
+    lib.rbp_mixed_replay.argtypes = [P, P]
+    lib.rbp_mixed_query.restype = ct.c_int
+    lib.rbp_mixed_query.argtypes = [P, i32, i32p, i32p, i32p, i32p]
     return lib
 
 

@@ -123,8 +123,11 @@ int layout_rows(int slots, int msg_type) {
 
 // Slot index of (slot j, check c) for the message type (slot_index<M> in the kernel).
 int slot_index_host(int j, int c, int C, int msg_type) {
-  const int vec = 16 / (int)msg_size(msg_type);
-  return (j / vec) * (vec * C) + c * vec + (j % vec);
+  switch (msg_type) {
+    case RBP_MSG_F32: return rbpk::slot_index<float>(j, c, C);
+    case RBP_MSG_F64: return rbpk::slot_index<double>(j, c, C);
+    default: return rbpk::slot_index<__half>(j, c, C);
+  }
 }
 
 // Block-wide tables first, then one region per group.
@@ -171,12 +174,27 @@ int vpt_for(int V, int G) {
   return -1;
 }
 
-// Default shape: the fewest threads per shot with at most 3 variables each
-// (rounded to whole warps, at most 1024), so a shot's iteration is short.
+// Default shape: the fewest owned variables per thread (from 3 up) whose group
+// still fits the register budget of that count, so a shot's iteration is short.
 int default_group_threads(int C, int V) {
-  int G = ((V + 2) / 3 + 31) / 32 * 32;
-  G = std::max(G, ((C + 31) / 32 + 31) / 32 * 32);
-  return std::min(std::max(G, 32), 1024);
+  for (int vpt : {3, 4, 6, 8, 12, 16}) {
+    const int G = std::max(32, (V + vpt - 1) / vpt + 31) / 32 * 32;
+    if (G <= rbpk::max_block_threads(vpt) && (C + G - 1) / G <= 32 && vpt_for(V, G) <= vpt) return G;
+  }
+  return 256;  // configure reports why no shape fits
+}
+
+// Allow a kernel the device's opt-in shared memory minus its static shared
+// memory as dynamic shared memory.  The attribute belongs to the kernel
+// function and is shared by every decoder using it, so it is set to that
+// limit; occupancy queries use each launch's actual size.
+cudaError_t set_max_dynamic_smem(const void* kernel, size_t max_smem, size_t* static_smem = nullptr) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if (static_smem) *static_smem = fa.sharedSizeBytes;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(max_smem - fa.sharedSizeBytes));
 }
 
 struct Launch {
@@ -211,9 +229,7 @@ int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, i
   if (NG < 1 || NG > max_groups)
     return fail(RBP_ERR_UNSUPPORTED,
                 w + ": groups_per_block must be in [1, " + std::to_string(max_groups) + "] for this shape");
-  // The attribute is per kernel function and shared by every decoder that uses
-  // this instantiation, so it is set to the device limit; occupancy uses `smem`.
-  RBP_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
+  RBP_CUDA(set_max_dynamic_smem(reinterpret_cast<const void*>(k), max_smem));
   const size_t smem = block_fixed + (size_t)NG * L.group_bytes;
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * NG, smem));
@@ -516,6 +532,272 @@ int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs
   const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks};
   return launch_decode(dgph, d->p, L, lc, d->llr.p, d->wunits.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
                        out, reinterpret_cast<cudaStream_t>(stream), "rbp_decode");
+}
+
+// ------------------------------------------------------------------ mixed-code launch
+
+}  // extern "C"
+
+struct rbp_mixed {
+  int n = 0;
+  int device = 0;
+  const rbp_decoder* dec[rbpk::kMaxMixedCodes] = {};
+  int G[rbpk::kMaxMixedCodes] = {}, NG[rbpk::kMaxMixedCodes] = {};
+  rbpk::MixedKernelFn kernel = nullptr;
+  int block_threads = 0, blocks = 0;
+  size_t smem = 0;
+  DevBuf<int> queues;
+  cudaStream_t capture_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~rbp_mixed() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (capture_stream) cudaStreamDestroy(capture_stream);
+  }
+};
+
+namespace {
+
+// Kernel arguments of one mixed launch.
+int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_outputs* outs, rbpk::MixedArgs* ma) {
+  std::memset(ma, 0, sizeof(*ma));
+  ma->ncodes = m->n;
+  double work[rbpk::kMaxMixedCodes] = {}, total = 0;
+  for (int i = 0; i < m->n; ++i) {
+    const rbp_decoder* d = m->dec[i];
+    const rbp_graph* g = d->g;
+    int rc = check_batch("rbp_mixed_decode", B[i], &ins[i], &outs[i], d->p, d->n_alpha);
+    if (rc != RBP_OK) return rc;
+    const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, m->G[i]);
+    ma->code[i].g = DevGraph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p,
+                             d->var_pos.p};
+    DevArgs& a = ma->code[i].a;
+    const rbp_params& p = d->p;
+    const rbp_batch* in = &ins[i];
+    const rbp_outputs* out = &outs[i];
+    a.pre_iter = in->pre_iter;
+    a.num_sets = p.num_sets;
+    a.set_max_iter = p.set_max_iter;
+    a.stop_nconv = p.stop_nconv;
+    a.last_leg = p.last_leg;
+    a.use_alpha = p.use_alpha;
+    a.use_beta = p.use_beta;
+    a.mix_mode = p.mix_mode;
+    a.skip_legs = in->skip_relay_legs;
+    a.beta = p.beta;
+    a.gamma0 = in->gamma0;
+    a.llr = d->llr.p;
+    a.wunits = d->wunits.p;
+    a.gamma_legs = d->gamma_legs.p;
+    a.alpha = d->alpha.p;
+    a.B = B[i];
+    a.syn = in->syndromes;
+    a.llr_shot = in->llr_per_shot;
+    a.gamma_pre = in->gamma_pre;
+    a.gamma_legs_shot = in->gamma_legs_shot;
+    a.n_shot_legs = in->n_shot_legs;
+    a.init_post = in->init_posterior;
+    a.errors = out->errors;
+    a.errors_packed = out->errors_packed;
+    a.weights = out->weights;
+    a.wfixed = reinterpret_cast<long long*>(out->weight_fixed);
+    a.found = out->found_count;
+    a.iters = out->iterations;
+    a.last_post = out->last_posterior;
+    a.queue = m->queues.p + i;
+    a.group_threads = m->G[i];
+    a.groups = m->NG[i];
+    a.off_chk_deg = L.off_chk_deg;
+    a.off_llr = L.off_llr;
+    a.off_group0 = L.off_group0;
+    a.group_bytes = L.group_bytes;
+    a.g_msg = L.g_msg;
+    a.g_hard = L.g_hard;
+    a.g_best = L.g_best;
+    a.g_first = L.g_first;
+    a.g_red = L.g_red;
+    work[i] = (double)B[i] * (double)g->E;
+    total += work[i];
+  }
+  // initial blocks per code in proportion to shots x edges; the kernel rebalances
+  double acc = 0;
+  for (int i = 0; i < m->n; ++i) {
+    ma->first_block[i] = (int)std::lround(total > 0 ? acc / total * m->blocks : 0);
+    acc += work[i];
+  }
+  ma->first_block[m->n] = m->blocks;
+  return RBP_OK;
+}
+
+int mixed_enqueue(rbp_mixed* m, const rbpk::MixedArgs& ma, cudaStream_t st) {
+  RBP_CUDA(cudaMemsetAsync(m->queues.p, 0, sizeof(int) * m->n, st));
+  m->kernel<<<m->blocks, m->block_threads, m->smem, st>>>(ma);
+  RBP_CUDA(cudaGetLastError());
+  return RBP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rbp_mixed_create(const rbp_decoder* const* decoders, int32_t n, rbp_mixed** out) {
+  if (!out) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_create: out is null");
+  *out = nullptr;
+  if (!decoders || n < 1 || n > rbpk::kMaxMixedCodes)
+    return fail(RBP_ERR_ARGUMENT, "rbp_mixed_create: between 1 and 8 decoders");
+  int vpt_need = 1, dc = 0, dv = 0;
+  for (int i = 0; i < n; ++i) {
+    const rbp_decoder* d = decoders[i];
+    if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_create: null decoder");
+    if (d->p.msg_type != RBP_MSG_F32)
+      return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_create: mixed launches use float32 messages");
+    if (d->g->device != decoders[0]->g->device)
+      return fail(RBP_ERR_ARGUMENT, "rbp_mixed_create: all decoders must be on one device");
+    dc = std::max(dc, d->g->slots);
+    dv = std::max(dv, d->g->vslots);
+    vpt_need = std::max(vpt_need, vpt_for(d->g->V, std::min(d->group_threads, 512)));
+  }
+  // The vectorised check pass moves MAXDC slots per row (8 or 16), so every
+  // code's padded layout must have exactly that many rows; codes whose rows
+  // differ cannot share a launch.  Beyond 16 the generic path reads each
+  // code's own degrees.
+  const int mixed_rows = dc <= 8 ? 8 : (dc <= 16 ? 16 : 0);
+  for (int i = 0; i < n && mixed_rows; ++i)
+    if (decoders[i]->rows != mixed_rows)
+      return fail(RBP_ERR_UNSUPPORTED,
+                  "rbp_mixed_create: codes with check degree <= 8 and 9..16 cannot share a launch");
+  // One instantiation serves every code: owned variables per thread VPT in
+  // {4, 8, 16}; a block of T threads (the register budget of VPT) holds, per
+  // code, as many groups as fit with at most VPT variables per thread.
+  int vpt = vpt_need <= 4 ? 4 : (vpt_need <= 8 ? 8 : 16);
+  rbp_mixed* m = new rbp_mixed();
+  m->n = n;
+  m->device = decoders[0]->g->device;
+  for (int i = 0; i < n; ++i) m->dec[i] = decoders[i];
+  DeviceGuard dg(m->device);
+  for (;; vpt *= 2) {
+    if (vpt > 16) {
+      delete m;
+      return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_create: a code needs more than 16 variables per thread");
+    }
+    const int T = rbpk::max_block_threads(vpt);
+    size_t smem = 0;
+    bool ok = true;
+    for (int i = 0; i < n && ok; ++i) {
+      const rbp_decoder* d = decoders[i];
+      const rbp_graph* g = d->g;
+      int best_G = 0, best_NG = 0;
+      for (int k = T / 32; k >= 1; --k) {  // most groups first
+        if ((T / k) % 32) continue;
+        const int Gc = T / k;
+        if (vpt_for(g->V, Gc) < 0 || vpt_for(g->V, Gc) > vpt || (g->C + Gc - 1) / Gc > 32) continue;
+        const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, Gc);
+        int ng = std::min(k, Gc == 32 ? k : 15);
+        while (ng >= 1 && (size_t)L.off_group0 + (size_t)ng * L.group_bytes > d->max_smem) --ng;
+        if (ng < 1) continue;
+        best_G = Gc;
+        best_NG = ng;
+        smem = std::max(smem, (size_t)L.off_group0 + (size_t)ng * L.group_bytes);
+        break;
+      }
+      if (!best_G) ok = false;
+      m->G[i] = best_G;
+      m->NG[i] = best_NG;
+    }
+    if (!ok) continue;
+    m->kernel = rbpk::pick_mixed_f32(dc, dv, vpt);
+    if (!m->kernel) {
+      delete m;
+      return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_create: no mixed kernel for these degrees");
+    }
+    m->block_threads = T;
+    m->smem = smem;
+    break;
+  }
+  size_t static_smem = 0;
+  cudaError_t e = set_max_dynamic_smem(reinterpret_cast<const void*>(m->kernel), decoders[0]->max_smem,
+                                       &static_smem);
+  if (e == cudaSuccess && m->smem + static_smem > decoders[0]->max_smem) e = cudaErrorInvalidValue;
+  int per_sm = 0;
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m->kernel, m->block_threads, m->smem);
+  if (e != cudaSuccess || per_sm < 1) {
+    delete m;
+    return fail(e != cudaSuccess ? RBP_ERR_CUDA : RBP_ERR_UNSUPPORTED,
+                std::string("rbp_mixed_create: occupancy: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "zero"));
+  }
+  m->blocks = per_sm * decoders[0]->sm_count;
+  int rc;
+  if ((rc = m->queues.upload(nullptr, n))) {
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return RBP_OK;
+}
+
+int rbp_mixed_destroy(rbp_mixed* m) {
+  if (!m) return RBP_OK;
+  DeviceGuard dg(m->device);
+  delete m;
+  return RBP_OK;
+}
+
+int rbp_mixed_decode(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_outputs* outs, void* stream) {
+  if (!m || !B || !ins || !outs) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_decode: null argument");
+  DeviceGuard dg(m->device);
+  rbpk::MixedArgs ma;
+  int rc = mixed_args(m, B, ins, outs, &ma);
+  if (rc != RBP_OK) return rc;
+  return mixed_enqueue(m, ma, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int rbp_mixed_capture(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_outputs* outs) {
+  if (!m || !B || !ins || !outs) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_capture: null argument");
+  DeviceGuard dg(m->device);
+  rbpk::MixedArgs ma;
+  int rc = mixed_args(m, B, ins, outs, &ma);
+  if (rc != RBP_OK) return rc;
+  if (!m->capture_stream) RBP_CUDA(cudaStreamCreateWithFlags(&m->capture_stream, cudaStreamNonBlocking));
+  if (m->exec) {
+    cudaGraphExecDestroy(m->exec);
+    m->exec = nullptr;
+  }
+  if (m->graph) {
+    cudaGraphDestroy(m->graph);
+    m->graph = nullptr;
+  }
+  RBP_CUDA(cudaStreamBeginCapture(m->capture_stream, cudaStreamCaptureModeThreadLocal));
+  rc = mixed_enqueue(m, ma, m->capture_stream);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(m->capture_stream, &graph);
+  if (rc != RBP_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(RBP_ERR_CUDA, std::string("rbp_mixed_capture: ") + cudaGetErrorString(e));
+  m->graph = graph;
+  RBP_CUDA(cudaGraphInstantiate(&m->exec, m->graph, 0));
+  return RBP_OK;
+}
+
+int rbp_mixed_replay(rbp_mixed* m, void* stream) {
+  if (!m) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_replay: null argument");
+  if (!m->exec) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_replay: nothing captured");
+  DeviceGuard dg(m->device);
+  RBP_CUDA(cudaGraphLaunch(m->exec, reinterpret_cast<cudaStream_t>(stream)));
+  return RBP_OK;
+}
+
+int rbp_mixed_query(const rbp_mixed* m, int32_t i, int32_t* group_threads, int32_t* groups_per_block,
+                    int32_t* block_threads, int32_t* blocks) {
+  if (!m || i < 0 || i >= m->n) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_query: bad arguments");
+  if (group_threads) *group_threads = m->G[i];
+  if (groups_per_block) *groups_per_block = m->NG[i];
+  if (block_threads) *block_threads = m->block_threads;
+  if (blocks) *blocks = m->blocks;
+  return RBP_OK;
 }
 
 // ------------------------------------------------------------------ decode without allocation

@@ -2,3 +2,4 @@
 #include "relaybp_kernel.cuh"
 
 RBPK_DEFINE_PICK(pick_f32, float)
+RBPK_DEFINE_PICK_MIXED(pick_mixed_f32, float)

@@ -73,11 +73,17 @@ struct MsgT<double> {
   static __device__ __forceinline__ double ld(double v) { return v; }
   static __device__ __forceinline__ double st(double v) { return v; }
 };
+// float16 messages saturate at the largest finite value (+-65504) before
+// rounding: posteriors with memory grow past float16's range on hard shots,
+// and an infinite message would turn the variable pass's inf - inf into NaN.
+__device__ __forceinline__ __half f16_saturate(float v) {
+  return __float2half_rn(fminf(fmaxf(v, -65504.0f), 65504.0f));
+}
 template <>
 struct MsgT<__half> {
   using A = float;
   static __device__ __forceinline__ float ld(__half v) { return __half2float(v); }
-  static __device__ __forceinline__ __half st(float v) { return __float2half_rn(v); }
+  static __device__ __forceinline__ __half st(float v) { return f16_saturate(v); }
 };
 template <>
 struct MsgT<__nv_bfloat16> {
@@ -188,16 +194,36 @@ struct DevArgs {
 enum HardSrc { HARD_ZERO = 0, HARD_POST = 1, HARD_BEST = 2 };
 constexpr uint16_t kNoSlot = 0xFFFFu;
 
-// Shared-memory index of slot j of check c.  The slots of a check are
-// contiguous in 16-byte chunks of VEC = 16 / sizeof(M) messages:
-//   index = (j / VEC) * (VEC * C) + c * VEC + j % VEC
-// so a check pass reads a row with 128-bit loads and consecutive checks are
-// consecutive chunks (a warp covers 512 contiguous bytes per chunk: no bank
-// conflicts).  The per-edge hard bytes use the same index.
+// Shared-memory index of slot j of check c.  The slots of a check sit in
+// 16-byte chunks of VEC = 16 / sizeof(M) messages, so a check pass moves a row
+// with 128-bit loads/stores and consecutive checks occupy consecutive chunks:
+//   index = (j / VEC) * (VEC * C) + c * VEC + ((j % VEC) ^ chunk_swizzle(c))
+// The XOR swizzle permutes the slots inside a chunk by bits 3-4 of c, so the
+// variable pass, whose warps touch the same slot of ~32 consecutive checks,
+// spreads those accesses over all 32 banks instead of 8.  The check pass's
+// work is symmetric in the slots of a row; it only needs the swizzle to know
+// which positions are padding.  The per-edge hard bytes use the same index.
+template <typename M>
+__host__ __device__ __forceinline__ int chunk_swizzle(int c) {
+  constexpr int VEC = 16 / (int)sizeof(M);
+  if constexpr (VEC == 8) return ((c >> 3) & 3) << 1;  // 16-bit messages: permute 4-byte words
+  else if constexpr (VEC == 4) return (c >> 3) & 3;
+  else return (c >> 3) & 1;
+}
+
 template <typename M>
 __host__ __device__ __forceinline__ int slot_index(int j, int c, int C) {
   constexpr int VEC = 16 / (int)sizeof(M);
-  return (j / VEC) * (VEC * C) + c * VEC + (j % VEC);
+  return (j / VEC) * (VEC * C) + c * VEC + ((j % VEC) ^ chunk_swizzle<M>(c));
+}
+
+// Index of the first element of chunk q of check c: the 16-byte aligned
+// address vector loads and stores use (physical element p of the chunk holds
+// slot q * VEC + (p ^ chunk_swizzle(c))).
+template <typename M>
+__host__ __device__ __forceinline__ int chunk_base(int q, int c, int C) {
+  constexpr int VEC = 16 / (int)sizeof(M);
+  return q * (VEC * C) + c * VEC;
 }
 
 // 16-byte vector access to VEC consecutive slots, converted to/from the
@@ -215,8 +241,10 @@ struct VecIO<float> {
   static __device__ __forceinline__ void store(float* p, const float* o) {
     *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
   }
-  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid) {
-    const uint32_t w = *reinterpret_cast<const uint32_t*>(p);
+  // Hard bytes of a chunk in logical slot order (XOR swizzle undone), the
+  // first `valid` kept: a word whose popcount parity is the chunk's parity.
+  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid, int swz) {
+    const uint32_t w = __byte_perm(*reinterpret_cast<const uint32_t*>(p), 0u, 0x3210u ^ (0x1111u * swz));
     return valid >= 4 ? w : (valid <= 0 ? 0u : w & ((1u << (8 * valid)) - 1u));
   }
 };
@@ -230,8 +258,9 @@ struct VecIO<double> {
   static __device__ __forceinline__ void store(double* p, const double* o) {
     *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
   }
-  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid) {
-    const uint32_t w = *reinterpret_cast<const uint16_t*>(p);
+  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid, int swz) {
+    uint32_t w = *reinterpret_cast<const uint16_t*>(p);
+    if (swz) w = ((w & 0xFFu) << 8) | (w >> 8);
     return valid >= 2 ? w : (valid <= 0 ? 0u : w & 0xFFu);
   }
 };
@@ -254,16 +283,19 @@ struct VecIO16 {
       w[i] = (uint32_t)Bits(FromF(o[2 * i])) | ((uint32_t)Bits(FromF(o[2 * i + 1])) << 16);
     *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
   }
-  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid) {
-    const uint2 w = *reinterpret_cast<const uint2*>(p);
-    const uint32_t lo = valid >= 4 ? w.x : (valid <= 0 ? 0u : w.x & ((1u << (8 * valid)) - 1u));
+  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid, int swz) {
+    const uint2 raw = *reinterpret_cast<const uint2*>(p);
+    const uint32_t sel = 0x3210u ^ (0x1111u * (swz & 2));
+    const uint32_t w0 = __byte_perm((swz & 4) ? raw.y : raw.x, 0u, sel);
+    const uint32_t w1 = __byte_perm((swz & 4) ? raw.x : raw.y, 0u, sel);
+    const uint32_t lo = valid >= 4 ? w0 : (valid <= 0 ? 0u : w0 & ((1u << (8 * valid)) - 1u));
     const int v2 = valid - 4;
-    const uint32_t hi = v2 >= 4 ? w.y : (v2 <= 0 ? 0u : w.y & ((1u << (8 * v2)) - 1u));
+    const uint32_t hi = v2 >= 4 ? w1 : (v2 <= 0 ? 0u : w1 & ((1u << (8 * v2)) - 1u));
     return lo ^ hi;
   }
 };
 __device__ __forceinline__ float h2f(__half h) { return __half2float(h); }
-__device__ __forceinline__ __half f2h(float f) { return __float2half_rn(f); }
+__device__ __forceinline__ __half f2h(float f) { return f16_saturate(f); }
 __device__ __forceinline__ unsigned short hbits(__half h) { return __half_as_ushort(h); }
 __device__ __forceinline__ __half hfrom(unsigned short b) { return __ushort_as_half(b); }
 __device__ __forceinline__ float b2f(__nv_bfloat16 h) { return __bfloat162float(h); }
@@ -299,18 +331,25 @@ __device__ __forceinline__ void ballot_post(const A (&post)[VPT], uint32_t* dst,
 // MAXDC check degree bound held in registers by the check pass (0: generic loop)
 // VPT   variables owned per thread
 // MAXDV variable degree bound (slot positions held in registers)
-template <typename M, int MAXDC, int VPT, int MAXDV>
-__global__ void __launch_bounds__(max_block_threads(VPT))
-relaybp_decode_kernel(DevGraph g, DevArgs a) {
-  using IO = MsgT<M>;
-  using A = typename IO::A;
-  extern __shared__ __align__(16) unsigned char smem[];
-
-  const int C = g.C, V = g.V;
+// Copy the code's block-wide tables (check degrees, prior LLRs) to shared memory.
+__device__ __forceinline__ void load_block_tables(const DevGraph& g, const DevArgs& a, unsigned char* smem) {
   uint8_t* s_chk_deg = smem + a.off_chk_deg;
   float* s_llr = reinterpret_cast<float*>(smem + a.off_llr);
-  for (int i = threadIdx.x; i < C; i += blockDim.x) s_chk_deg[i] = g.chk_deg[i];
-  for (int i = threadIdx.x; i < V; i += blockDim.x) s_llr[i] = a.llr[i];
+  for (int i = threadIdx.x; i < g.C; i += blockDim.x) s_chk_deg[i] = g.chk_deg[i];
+  for (int i = threadIdx.x; i < g.V; i += blockDim.x) s_llr[i] = a.llr[i];
+}
+
+// The groups of this block decode shots of one code until its work queue is
+// empty.  The block-wide tables must be in shared memory (load_block_tables +
+// a block barrier); threads beyond a.groups * a.group_threads return at once.
+template <typename M, int MAXDC, int VPT, int MAXDV>
+__device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, unsigned char* smem) {
+  using IO = MsgT<M>;
+  using A = typename IO::A;
+
+  const int C = g.C, V = g.V;
+  const uint8_t* s_chk_deg = smem + a.off_chk_deg;
+  const float* s_llr = reinterpret_cast<const float*>(smem + a.off_llr);
 
   const int G = a.group_threads;
   const int gid = threadIdx.x / G;
@@ -322,26 +361,20 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
   const int W = (V + 31) >> 5;
   const int S = a.stop_nconv;
 
-  // slot positions of the owned variables' edges, two 16-bit slots per word;
-  // absent edges (degree < MAXDV) point at the dummy slot after the last row
+  // slot positions of the owned variables' edges in summation order; absent
+  // edges (degree < MAXDV) point at the dummy slot after the last row
   const uint32_t dummy = (uint32_t)(g.rows * C);
-  uint32_t vpos[VPT][(MAXDV + 1) / 2];
+  uint32_t vpos[VPT][MAXDV];
 #pragma unroll
   for (int k = 0; k < VPT; ++k) {
     const int v = t + k * G;
 #pragma unroll
-    for (int j = 0; j < (MAXDV + 1) / 2; ++j) {
-      uint32_t lo = dummy, hi = dummy;
-      if (v < V) {
-        if (2 * j < g.vslots) lo = g.var_pos[(2 * j) * V + v];
-        if (2 * j + 1 < g.vslots) hi = g.var_pos[(2 * j + 1) * V + v];
-      }
-      lo = lo == kNoSlot ? dummy : lo;
-      hi = hi == kNoSlot ? dummy : hi;
-      vpos[k][j] = lo | (hi << 16);
+    for (int j = 0; j < MAXDV; ++j) {
+      uint32_t p = dummy;
+      if (v < V && j < g.vslots) p = g.var_pos[j * V + v];
+      vpos[k][j] = p == kNoSlot ? dummy : p;
     }
   }
-  __syncthreads();
   if (gid >= a.groups) return;
 
   unsigned char* gsm = smem + a.off_group0 + gid * a.group_bytes;
@@ -420,7 +453,7 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
             gam[k] = grow ? A(__ldg(grow + v)) : A(gs);
             const M m0 = IO::st(llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]));
 #pragma unroll
-            for (int j = 0; j < MAXDV; ++j) msg[(vpos[k][j >> 1] >> ((j & 1) * 16)) & 0xFFFFu] = m0;
+            for (int j = 0; j < MAXDV; ++j) msg[vpos[k][j]] = m0;
           }
         }
         group_sync(bar, G);
@@ -442,16 +475,18 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
               // The row's slots are contiguous in 16-byte chunks (VEC messages each)
               // and padded to MAXDC: NQ vector loads/stores, padding masked by selects.
               constexpr int NQ = MAXDC / VecIO<M>::N;
+              constexpr int VEC = VecIO<M>::N;
               const int deg = s_chk_deg[c];
+              const int swz = chunk_swizzle<M>(c);
               A mv[MAXDC];
 #pragma unroll
               for (int q = 0; q < NQ; ++q)
-                VecIO<M>::load(msg + slot_index<M>(q * VecIO<M>::N, c, C), mv + q * VecIO<M>::N);
+                VecIO<M>::load(msg + chunk_base<M>(q, c, C), mv + q * VecIO<M>::N);
               if (check_parity) {
                 uint32_t x = 0;
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                  x ^= VecIO<M>::hard_word(hard + slot_index<M>(q * VecIO<M>::N, c, C), deg - q * VecIO<M>::N);
+                  x ^= VecIO<M>::hard_word(hard + chunk_base<M>(q, c, C), deg - q * VEC, swz);
                 ok_all = ok_all && ((__popc(x) & 1) == s);
               }
               if (write_nu) {
@@ -462,7 +497,8 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
                 const A kInf = A(__int_as_float(0x7f800000));
 #pragma unroll
                 for (int j = 0; j < MAXDC; ++j) {
-                  const bool in = j < deg;
+                  // physical position j holds slot (j / VEC) * VEC + ((j % VEC) ^ swz)
+                  const bool in = ((j % VEC) ^ swz) < deg - (j / VEC) * VEC;
                   neg ^= (in && mv[j] < A(0)) ? 1 : 0;  // parity of negative messages (kernels.py:1134)
                   const A x = in ? fmin(fabs(mv[j]), kInf) : kInf;
                   min2 = fmin(min2, fmax(min1, x));
@@ -489,7 +525,7 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
                 }
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
-                  VecIO<M>::store(msg + slot_index<M>(q * VecIO<M>::N, c, C), out + q * VecIO<M>::N);
+                  VecIO<M>::store(msg + chunk_base<M>(q, c, C), out + q * VecIO<M>::N);
               }
             } else {
               const int deg = g.chk_ptr[c + 1] - g.chk_ptr[c];
@@ -567,7 +603,7 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
               A sum = A(0);
 #pragma unroll
               for (int j = 0; j < MAXDV; ++j) {
-                const uint32_t p = (vpos[kk][j >> 1] >> ((j & 1) * 16)) & 0xFFFFu;
+                const uint32_t p = vpos[kk][j];
                 nv[j] = IO::ld(msg[p]);
                 // absent edges point at the group's dummy slot and are not summed
                 sum = (p != dummy) ? add_rn(sum, nv[j]) : sum;
@@ -577,7 +613,7 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
               const uint8_t h = pv <= A(0) ? 1 : 0;
 #pragma unroll
               for (int j = 0; j < MAXDV; ++j) {
-                const uint32_t p = (vpos[kk][j >> 1] >> ((j & 1) * 16)) & 0xFFFFu;
+                const uint32_t p = vpos[kk][j];
                 msg[p] = IO::st(add_rn(lm, sub_rn(sum, nv[j])));
                 hard[p] = h;
               }
@@ -656,6 +692,62 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
   }
 }
 
+// One code, one launch (rbp_decode, rbp_decode_static).
+template <typename M, int MAXDC, int VPT, int MAXDV>
+__global__ void __launch_bounds__(max_block_threads(VPT))
+relaybp_decode_kernel(DevGraph g, DevArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  load_block_tables(g, a, smem);
+  __syncthreads();
+  run_groups<M, MAXDC, VPT, MAXDV>(g, a, smem);
+}
+
+// Several codes in one launch (rbp_mixed_*).  Block b starts on the code whose
+// block range holds b (first_block[], from the host's work estimate).  When
+// that code's queue is empty the whole block moves to the next code that still
+// has shots, re-partitioning its threads into that code's group shape, until
+// every queue is empty.  Queue counters only grow, so the loop ends.
+constexpr int kMaxMixedCodes = 8;
+
+struct MixedCode {
+  DevGraph g;
+  DevArgs a;
+};
+
+struct MixedArgs {
+  MixedCode code[kMaxMixedCodes];
+  int ncodes;
+  int first_block[kMaxMixedCodes + 1];
+};
+
+template <typename M, int MAXDC, int VPT, int MAXDV>
+__global__ void __launch_bounds__(max_block_threads(VPT))
+relaybp_mixed_kernel(const __grid_constant__ MixedArgs m) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_next;
+  int code = 0;
+  while (code + 1 < m.ncodes && (int)blockIdx.x >= m.first_block[code + 1]) ++code;
+  while (code >= 0) {
+    const DevGraph g = m.code[code].g;
+    const DevArgs a = m.code[code].a;
+    load_block_tables(g, a, smem);
+    __syncthreads();
+    run_groups<M, MAXDC, VPT, MAXDV>(g, a, smem);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int next = -1;
+      for (int i = 1; i <= m.ncodes && next < 0; ++i) {
+        const int c = (code + i) % m.ncodes;
+        if (*reinterpret_cast<volatile const int*>(m.code[c].a.queue) < m.code[c].a.B) next = c;
+      }
+      s_next = next;
+    }
+    __syncthreads();
+    code = s_next;
+    __syncthreads();
+  }
+}
+
 using KernelFn = void (*)(DevGraph, DevArgs);
 
 // Kernel for (check degree bound, variable degree, owned variables per thread),
@@ -664,6 +756,9 @@ KernelFn pick_f32(int dc, int dv, int vpt);
 KernelFn pick_f16(int dc, int dv, int vpt);
 KernelFn pick_bf16(int dc, int dv, int vpt);
 KernelFn pick_f64(int dc, int dv, int vpt);
+
+using MixedKernelFn = void (*)(MixedArgs);
+MixedKernelFn pick_mixed_f32(int dc, int dv, int vpt);
 
 // Supported owned-variable counts, ascending.
 constexpr int kVptChoices[] = {1, 2, 3, 4, 6, 8, 12, 16};
@@ -679,6 +774,23 @@ constexpr int kVptChoices[] = {1, 2, 3, 4, 6, 8, 12, 16};
   if (dc <= 8) { RBPK_DC_DV(M, 8, VPT) }                                       \
   if (dc <= 16) { RBPK_DC_DV(M, 16, VPT) }                                     \
   { RBPK_DC_DV(M, 0, VPT) }
+#define RBPK_MDC_DV(M, DC, VPT)                                                \
+  if (dv <= 3) return &rbpk::relaybp_mixed_kernel<M, DC, VPT, 3>;              \
+  if (dv <= 8) return &rbpk::relaybp_mixed_kernel<M, DC, VPT, 8>;              \
+  return nullptr;
+#define RBPK_MDC(M, VPT)                                                       \
+  if (dc <= 8) { RBPK_MDC_DV(M, 8, VPT) }                                      \
+  if (dc <= 16) { RBPK_MDC_DV(M, 16, VPT) }                                    \
+  { RBPK_MDC_DV(M, 0, VPT) }
+#define RBPK_DEFINE_PICK_MIXED(NAME, M)                                        \
+  rbpk::MixedKernelFn rbpk::NAME(int dc, int dv, int vpt) {                    \
+    switch (vpt) {                                                             \
+      case 4: { RBPK_MDC(M, 4) }                                               \
+      case 8: { RBPK_MDC(M, 8) }                                               \
+      case 16: { RBPK_MDC(M, 16) }                                             \
+      default: return nullptr;                                                 \
+    }                                                                          \
+  }
 #define RBPK_DEFINE_PICK(NAME, M)                                              \
   rbpk::KernelFn rbpk::NAME(int dc, int dv, int vpt) {                         \
     switch (vpt) {                                                             \
