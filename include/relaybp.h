@@ -127,6 +127,17 @@ typedef struct {
   int32_t n_shot_legs;
   int32_t pre_iter;                /* first-phase iterations for this call (pre_iter_override) */
   int32_t skip_relay_legs;         /* 1: stop after the first phase */
+  /* Resumable decoding (rbp_state_bytes bytes per shot, device memory).  With
+   * resume_state, each shot continues from its saved state at relay leg
+   * legs_begin instead of starting with the pre-iterations; relay legs run up to
+   * (excluding) legs_end (<= 0: all).  With suspend_state, each shot's state
+   * after the last phase run is saved.  The two may be the same buffer; both
+   * must be 16-byte aligned.  No reference counterpart: the reference's
+   * fast_max_unconverged_pct exit (decoder.py:2890-2935) is built on it. */
+  const void* resume_state;
+  void* suspend_state;
+  int32_t legs_begin;
+  int32_t legs_end;
 } rbp_batch;
 
 /* Outputs (device memory).  Any may be NULL except found_count/iterations. */
@@ -139,6 +150,9 @@ typedef struct {
   int32_t* iterations;             /* [B] BP iterations the shot ran */
   void* last_posterior;            /* [B, V] f32 (f64 for RBP_MSG_F64) posterior at the end */
 } rbp_outputs;
+
+/* Bytes of one shot's saved state (rbp_batch.resume_state / suspend_state). */
+RBP_API int rbp_state_bytes(const rbp_decoder* d, int64_t* bytes_per_shot);
 
 /*
  * Decode B shots on `stream`.  Asynchronous: returns after the launch.

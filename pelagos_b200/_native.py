@@ -39,6 +39,7 @@ EXPORTED_SYMBOLS = (
     "rbp_decoder_set_llr",
     "rbp_decoder_configure",
     "rbp_decoder_query",
+    "rbp_state_bytes",
     "rbp_decode",
     "rbp_decode_static",
     "rbp_mixed_create",
@@ -83,6 +84,10 @@ class RbpBatch(ct.Structure):
         ("n_shot_legs", ct.c_int32),
         ("pre_iter", ct.c_int32),
         ("skip_relay_legs", ct.c_int32),
+        ("resume_state", ct.c_void_p),
+        ("suspend_state", ct.c_void_p),
+        ("legs_begin", ct.c_int32),
+        ("legs_end", ct.c_int32),
     ]
 
 
@@ -124,6 +129,8 @@ def _declare(lib):
     lib.rbp_decoder_configure.argtypes = [P, i32, i32]
     lib.rbp_decoder_query.restype = ct.c_int
     lib.rbp_decoder_query.argtypes = [P, ct.POINTER(i64), ct.POINTER(i64), i32p, i32p, i32p]
+    lib.rbp_state_bytes.restype = ct.c_int
+    lib.rbp_state_bytes.argtypes = [P, ct.POINTER(i64)]
     lib.rbp_decode.restype = ct.c_int
     lib.rbp_decode.argtypes = [P, i64, ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs), P]
     lib.rbp_decode_static.restype = ct.c_int

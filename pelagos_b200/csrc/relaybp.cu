@@ -250,6 +250,10 @@ int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outpu
   if (p.use_alpha && in->pre_iter > n_alpha) return fail(RBP_ERR_ARGUMENT, w + ": pre_iter exceeds the alpha table");
   if (in->n_shot_legs < 0 || (in->n_shot_legs > 0 && !in->gamma_legs_shot))
     return fail(RBP_ERR_ARGUMENT, w + ": gamma_legs_shot missing");
+  if (in->resume_state && (in->legs_begin < 0 || in->legs_begin > p.num_sets))
+    return fail(RBP_ERR_ARGUMENT, w + ": legs_begin out of range");
+  if ((reinterpret_cast<uintptr_t>(in->resume_state) | reinterpret_cast<uintptr_t>(in->suspend_state)) % 16)
+    return fail(RBP_ERR_ARGUMENT, w + ": resume_state and suspend_state must be 16-byte aligned");
   return RBP_OK;
 }
 
@@ -287,6 +291,11 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.found = out->found_count;
   a.iters = out->iterations;
   a.last_post = out->last_posterior;
+  a.legs_begin = in->legs_begin;
+  a.legs_end = in->legs_end;
+  a.resume = static_cast<const unsigned char*>(in->resume_state);
+  a.suspend = static_cast<unsigned char*>(in->suspend_state);
+  a.state_stride = rbpk::state_stride(dgph.V, p.msg_type == RBP_MSG_F64 ? 8 : 4);
   a.queue = queue;
   a.group_threads = lc.group_threads;
   a.groups = lc.groups;
@@ -509,6 +518,12 @@ int rbp_decoder_destroy(rbp_decoder* d) {
   return RBP_OK;
 }
 
+int rbp_state_bytes(const rbp_decoder* d, int64_t* bytes_per_shot) {
+  if (!d || !bytes_per_shot) return fail(RBP_ERR_ARGUMENT, "rbp_state_bytes: null argument");
+  *bytes_per_shot = rbpk::state_stride(d->g->V, d->p.msg_type == RBP_MSG_F64 ? 8 : 4);
+  return RBP_OK;
+}
+
 int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem, int32_t* group_threads,
                       int32_t* groups_per_block, int32_t* blocks) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_query: null decoder");
@@ -605,6 +620,11 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.found = out->found_count;
     a.iters = out->iterations;
     a.last_post = out->last_posterior;
+    a.legs_begin = in->legs_begin;
+    a.legs_end = in->legs_end;
+    a.resume = static_cast<const unsigned char*>(in->resume_state);
+    a.suspend = static_cast<unsigned char*>(in->suspend_state);
+    a.state_stride = rbpk::state_stride(g->V, 4);
     a.queue = m->queues.p + i;
     a.group_threads = m->G[i];
     a.groups = m->NG[i];

@@ -183,6 +183,12 @@ struct DevArgs {
   int* found;
   int* iters;
   void* last_post;
+  // resumable decoding: shot state after/before a phase (see ShotStateLayout)
+  int legs_begin;                // first relay leg when resuming
+  int legs_end;                  // relay legs < legs_end run (<= 0: all)
+  const unsigned char* resume;   // [B, state_stride] or null: start from the pre-iterations
+  unsigned char* suspend;        // [B, state_stride] or null
+  int state_stride;
   // scheduling
   int* queue;
   int group_threads, groups;
@@ -192,6 +198,16 @@ struct DevArgs {
 };
 
 enum HardSrc { HARD_ZERO = 0, HARD_POST = 1, HARD_BEST = 2 };
+
+// Per-shot decode state between launches (bytes):
+//   [0,4) found  [4,8) iterations  [8,12) hard source  [12,16) has-best
+//   [16,24) best weight (2^-32 units)  [24,32) unused
+//   [32, 32+4W) best-solution bits, [32+4W, 32+8W) first-leg bits,
+//   then the posterior [V] (accumulation type) at post_offset.
+__host__ __device__ constexpr int state_post_offset(int V) { return (32 + 8 * ((V + 31) / 32) + 15) / 16 * 16; }
+__host__ __device__ constexpr int state_stride(int V, int acc_bytes) {
+  return (state_post_offset(V) + acc_bytes * V + 15) / 16 * 16;
+}
 constexpr uint16_t kNoSlot = 0xFFFFu;
 
 // Shared-memory index of slot j of check c.  The slots of a check sit in
@@ -403,28 +419,51 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
       for (int c = t; c < C; c += G, ++k) synm |= (uint32_t)(syn_row[c] & 1) << k;
     }
     const float* llr_row = a.llr_shot ? a.llr_shot + b * (long long)V : nullptr;
-#pragma unroll
-    for (int k = 0; k < VPT; ++k) {
-      const int v = t + k * G;
-      A p0 = A(0);
-      if (v < V) {
-        if (a.init_post) p0 = A(__ldg(a.init_post + b * (long long)V + v));
-        else p0 = llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]);
-      }
-      post[k] = p0;
-    }
-    for (int w = t; w < W; w += G) {
-      best_bits[w] = 0u;
-      first_bits[w] = 0u;
-    }
     long long best_w = LLONG_MAX;
     int found = 0, iters = 0, hard_src = HARD_ZERO, sought = 1;
     bool has_best = false;
     const int pre = a.pre_iter;
+    if (a.resume) {
+      // continue a shot suspended after an earlier phase
+      const unsigned char* st = a.resume + b * (long long)a.state_stride;
+      const int* hdr = reinterpret_cast<const int*>(st);
+      found = hdr[0];
+      iters = hdr[1];
+      hard_src = hdr[2];
+      has_best = hdr[3] != 0;
+      best_w = *reinterpret_cast<const long long*>(st + 16);
+      const uint32_t* bits = reinterpret_cast<const uint32_t*>(st + 32);
+      for (int w = t; w < W; w += G) {
+        best_bits[w] = bits[w];
+        first_bits[w] = bits[W + w];
+      }
+      const A* sp = reinterpret_cast<const A*>(st + state_post_offset(V));
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) {
+        const int v = t + k * G;
+        post[k] = v < V ? sp[v] : A(0);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) {
+        const int v = t + k * G;
+        A p0 = A(0);
+        if (v < V) {
+          if (a.init_post) p0 = A(__ldg(a.init_post + b * (long long)V + v));
+          else p0 = llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]);
+        }
+        post[k] = p0;
+      }
+      for (int w = t; w < W; w += G) {
+        best_bits[w] = 0u;
+        first_bits[w] = 0u;
+      }
+    }
+    const int legs_stop = (a.legs_end > 0 && a.legs_end < a.num_sets) ? a.legs_end : a.num_sets;
 
     // Phase -1: the pre-iterations (decoder.py:3480-3616); phase l >= 0: relay
-    // leg l (decoder.py:3672-3837).
-    for (int phase = -1; phase < a.num_sets; ++phase) {
+    // leg l (decoder.py:3672-3837).  A resumed shot starts at leg legs_begin.
+    for (int phase = a.resume ? a.legs_begin : -1; phase < legs_stop; ++phase) {
       int max_iter;
       const float* grow;
       float gs = 0.f;
@@ -641,6 +680,28 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
 
     // ---------------- outputs, decoder.py:3839-3873
     group_sync(bar, G);
+    if (a.suspend) {
+      unsigned char* st = a.suspend + b * (long long)a.state_stride;
+      if (t == 0) {
+        int* hdr = reinterpret_cast<int*>(st);
+        hdr[0] = found;
+        hdr[1] = iters;
+        hdr[2] = hard_src;
+        hdr[3] = has_best ? 1 : 0;
+        *reinterpret_cast<long long*>(st + 16) = best_w;
+      }
+      uint32_t* bits = reinterpret_cast<uint32_t*>(st + 32);
+      for (int w = t; w < W; w += G) {
+        bits[w] = best_bits[w];
+        bits[W + w] = first_bits[w];
+      }
+      A* sp = reinterpret_cast<A*>(st + state_post_offset(V));
+#pragma unroll
+      for (int k = 0; k < VPT; ++k) {
+        const int v = t + k * G;
+        if (v < V) sp[v] = post[k];
+      }
+    }
     const uint32_t* src_bits = has_best ? best_bits : first_bits;
     const bool from_post = !has_best && a.last_leg && hard_src == HARD_POST;
     const bool zero_bits = !has_best && a.last_leg && hard_src != HARD_POST;

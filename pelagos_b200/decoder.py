@@ -15,8 +15,10 @@ Differences from the reference, by design:
   lowest-weight selection does not depend on a summation order;
 * results are fresh tensors (the reference returns views of per-batch-size
   cached buffers that the next decode overwrites);
-* ``scheduling="layered"`` and ``fast_max_unconverged_pct`` are not provided
-  (they need leg-synchronous batches; the kernel retires each shot on its own).
+* ``scheduling="layered"`` is not provided;
+* ``fast_max_unconverged_pct`` decodes leg-synchronously (one launch per leg,
+  each resuming the shots' saved state), since its early exit is a batch-level
+  decision; every other call runs all legs in one launch.
 """
 
 from __future__ import annotations
@@ -195,10 +197,7 @@ class RelayBPDecoder:
             if not (0.0 <= fast_max_unconverged_pct <= 1.0):
                 raise ValueError(
                     f"fast_max_unconverged_pct must be between 0.0 and 1.0, got {fast_max_unconverged_pct}")
-            raise NotImplementedError(
-                "fast_max_unconverged_pct needs leg-synchronous batches; this decoder retires each shot "
-                "independently inside one kernel")
-        self.fast_max_unconverged_pct = None
+        self.fast_max_unconverged_pct = fast_max_unconverged_pct
         self.normalized_min_sum_alpha = normalized_min_sum_alpha
         self.offset_min_sum_beta = offset_min_sum_beta
 
@@ -455,6 +454,9 @@ class RelayBPDecoder:
                 self._native[g] = self._make_native(g, self._alpha_len)
 
         if self.num_gpus == 1:
+            if self.fast_max_unconverged_pct is not None and not skip_relay_legs:
+                return self._decode_leg_synchronous(syndromes, pre, init_posterior, init_gamma,
+                                                    return_last_posterior, prior_llr, leg_gammas)
             return self._decode_on(self.device_ids[0], syndromes, 0, pre, init_posterior, init_gamma,
                                    skip_relay_legs, return_last_posterior, prior_llr, leg_gammas)
         splits = self._split_batch(B, self.num_gpus)
@@ -485,8 +487,55 @@ class RelayBPDecoder:
         out["unconverged_indices"] = torch.cat(unc, 0).to(torch.int32)
         return out
 
+    def state_bytes(self) -> int:
+        """Bytes of one shot's saved decode state (resumable decoding)."""
+        b = ct.c_int64()
+        nat.check(nat.lib().rbp_state_bytes(self._native[self.device_ids[0]]._dec, ct.byref(b)), "rbp_state_bytes")
+        return int(b.value)
+
+    def new_state(self, B: int) -> torch.Tensor:
+        """Device buffer for B shots' saved decode state."""
+        return torch.empty(B, self.state_bytes(), dtype=torch.uint8, device=self._device_strs[self.device_ids[0]])
+
+    def decode_phases(self, syndromes: torch.Tensor, *, resume: Optional[torch.Tensor] = None,
+                      suspend: Optional[torch.Tensor] = None, legs_begin: int = 0, legs_end: int = 0,
+                      skip_relay_legs: bool = False, leg_gammas: Optional[torch.Tensor] = None,
+                      return_last_posterior: bool = False) -> Dict[str, torch.Tensor]:
+        """Run part of a decode: from the pre-iterations (or, with `resume`, from relay leg
+        `legs_begin` of the saved state) up to relay leg `legs_end` (0: all), saving the state in
+        `suspend`.  Outputs reflect the shots' state after the last phase run."""
+        if self.num_gpus != 1:
+            raise ValueError("resumable decoding runs on one GPU")
+        if resume is not None and not 0 <= legs_begin <= self.num_sets:
+            raise ValueError("legs_begin out of range")
+        return self._decode_on(self.device_ids[0], syndromes, 0, self.pre_iter, None, None, skip_relay_legs,
+                               return_last_posterior, None, leg_gammas, resume, suspend, legs_begin, legs_end)
+
+    def _decode_leg_synchronous(self, syndromes, pre, init_posterior, init_gamma, return_last_posterior,
+                                prior_llr, leg_gammas):
+        """decode() with fast_max_unconverged_pct: the pre-iterations, then one relay leg per launch,
+        checking after each phase, as the reference does (decoder.py:3619-3662, 3812-3831), whether
+        every shot is done or the unconverged fraction fell below the threshold."""
+        gid = self.device_ids[0]
+        B = int(syndromes.shape[0])
+        state = self.new_state(B)
+        out = self._decode_on(gid, syndromes, 0, pre, init_posterior, init_gamma, True,
+                              return_last_posterior, prior_llr, leg_gammas, None, state, 0, 0)
+        thr = self.fast_max_unconverged_pct
+        for leg in range(-1, self.num_sets):
+            if leg >= 0:
+                out = self._decode_on(gid, syndromes, 0, pre, None, None, False, return_last_posterior,
+                                      prior_llr, leg_gammas, state, state, leg, leg + 1)
+            unconv = float((out["found_count"] < self.stop_nconv).float().mean()) if B else 0.0
+            if unconv == 0.0:
+                break
+            if unconv < thr and unconv < 1.0:
+                break
+        return out
+
     def _decode_on(self, gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
-                   return_last_posterior, prior_llr, leg_gammas) -> Dict[str, torch.Tensor]:
+                   return_last_posterior, prior_llr, leg_gammas, resume=None, suspend=None, legs_begin=0,
+                   legs_end=0) -> Dict[str, torch.Tensor]:
         B = int(syndromes.shape[0])
         dev = self._device_strs[gpu_id]
         with torch.cuda.device(gpu_id):
@@ -525,7 +574,9 @@ class RelayBPDecoder:
             batch = nat.RbpBatch(syndromes=_ptr(syn), llr_per_shot=_ptr(pl), gamma_pre=_ptr(ig),
                                  gamma0=gamma0, init_posterior=_ptr(ip), gamma_legs_shot=_ptr(shot_legs),
                                  n_shot_legs=n_shot_legs, pre_iter=pre,
-                                 skip_relay_legs=1 if skip_relay_legs else 0)
+                                 skip_relay_legs=1 if skip_relay_legs else 0,
+                                 resume_state=_ptr(resume), suspend_state=_ptr(suspend),
+                                 legs_begin=int(legs_begin), legs_end=int(legs_end))
             outs = nat.RbpOutputs(errors=_ptr(errors), errors_packed=_ptr(packed), weights=None,
                                   weight_fixed=_ptr(wfix), found_count=_ptr(found), iterations=_ptr(iters),
                                   last_posterior=_ptr(last_post))
