@@ -123,7 +123,7 @@ typedef struct {
   const float* gamma_pre;          /* [B, V] init_gamma for the first phase */
   float gamma0;                    /* first-phase strength when gamma_pre is NULL (0 for algo=plain) */
   const float* init_posterior;     /* [B, V] posterior the first phase starts from */
-  const float* gamma_legs_shot;    /* [B, n_shot_legs, V] per-shot strengths of legs < n_shot_legs */
+  const float* gamma_legs_shot;    /* [B, shot_leg_rows, V] per-shot strengths of legs < n_shot_legs */
   int32_t n_shot_legs;
   int32_t pre_iter;                /* first-phase iterations for this call (pre_iter_override) */
   int32_t skip_relay_legs;         /* 1: stop after the first phase */
@@ -138,6 +138,9 @@ typedef struct {
   void* suspend_state;
   int32_t legs_begin;
   int32_t legs_end;
+  /* Rows per shot in gamma_legs_shot (0: n_shot_legs).  Leg l < n_shot_legs
+   * uses row min(l, shot_leg_rows - 1), so one row can serve several legs. */
+  int32_t shot_leg_rows;
 } rbp_batch;
 
 /* Outputs (device memory).  Any may be NULL except found_count/iterations. */

@@ -88,6 +88,18 @@ class RbpBatch(ct.Structure):
         ("suspend_state", ct.c_void_p),
         ("legs_begin", ct.c_int32),
         ("legs_end", ct.c_int32),
+        ("shot_leg_rows", ct.c_int32),
+    ]
+
+
+class RbpNetHparams(ct.Structure):
+    _fields_ = [
+        ("lr", ct.c_float),
+        ("beta1", ct.c_float),
+        ("beta2", ct.c_float),
+        ("eps", ct.c_float),
+        ("weight_decay", ct.c_float),
+        ("w_neg", ct.c_float),
     ]
 
 

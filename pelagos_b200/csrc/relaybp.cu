@@ -3,6 +3,7 @@
 // itself is in relaybp_kernel.cuh.
 
 #include "relaybp.h"
+#include "relaybp_host.h"
 #include "relaybp_kernel.cuh"
 
 #include <cuda_runtime.h>
@@ -20,70 +21,19 @@ namespace {
 using rbpk::DevArgs;
 using rbpk::DevGraph;
 using rbpk::KernelFn;
-
-thread_local std::string g_err;
-
-int fail(int code, const std::string& msg) {
-  g_err = msg;
-  return code;
-}
-
-#define RBP_CUDA(expr)                                                                      \
-  do {                                                                                       \
-    cudaError_t e_ = (expr);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
-      return fail(RBP_ERR_CUDA, std::string(#expr) + " failed: " + cudaGetErrorString(e_));  \
-  } while (0)
-
-// Restores the caller's current device on scope exit.
-struct DeviceGuard {
-  int prev = -1;
-  bool ok = false;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(dev) == cudaSuccess) ok = true;
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
-
-inline int align16(int x) { return (x + 15) & ~15; }
-
-// ------------------------------------------------------------------ host objects
-
-template <typename T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DevBuf() = default;
-  DevBuf(const DevBuf&) = delete;
-  DevBuf& operator=(const DevBuf&) = delete;
-  ~DevBuf() {
-    if (p) cudaFree(p);
-  }
-  int upload(const T* host, size_t count) {
-    if (p) {
-      cudaFree(p);
-      p = nullptr;
-    }
-    n = count;
-    if (count == 0) return RBP_OK;
-    RBP_CUDA(cudaMalloc(&p, count * sizeof(T)));
-    if (host) RBP_CUDA(cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice));
-    return RBP_OK;
-  }
-};
+using rbph::align16;
+using rbph::DevBuf;
+using rbph::DeviceGuard;
+using rbph::fail;
 
 }  // namespace
 
-struct rbp_graph {
-  int device = 0;
-  int C = 0, V = 0, E = 0, slots = 0, vslots = 0;
-  // host copy of the edge-centric graph (slot positions depend on the message type)
-  std::vector<int> edge_chk, edge_slot, var_ptr, var_edges;
-  DevBuf<uint8_t> chk_deg;
-  DevBuf<int> chk_ptr;
-};
+namespace rbph {
+std::string& err_slot() {
+  thread_local std::string s;
+  return s;
+}
+}  // namespace rbph
 
 struct rbp_decoder {
   const rbp_graph* g = nullptr;
@@ -250,6 +200,7 @@ int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outpu
   if (p.use_alpha && in->pre_iter > n_alpha) return fail(RBP_ERR_ARGUMENT, w + ": pre_iter exceeds the alpha table");
   if (in->n_shot_legs < 0 || (in->n_shot_legs > 0 && !in->gamma_legs_shot))
     return fail(RBP_ERR_ARGUMENT, w + ": gamma_legs_shot missing");
+  if (in->shot_leg_rows < 0) return fail(RBP_ERR_ARGUMENT, w + ": shot_leg_rows must be >= 0");
   if (in->resume_state && (in->legs_begin < 0 || in->legs_begin > p.num_sets))
     return fail(RBP_ERR_ARGUMENT, w + ": legs_begin out of range");
   if ((reinterpret_cast<uintptr_t>(in->resume_state) | reinterpret_cast<uintptr_t>(in->suspend_state)) % 16)
@@ -283,6 +234,7 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.gamma_pre = in->gamma_pre;
   a.gamma_legs_shot = in->gamma_legs_shot;
   a.n_shot_legs = in->n_shot_legs;
+  a.shot_leg_rows = in->shot_leg_rows > 0 ? in->shot_leg_rows : std::max(1, in->n_shot_legs);
   a.init_post = in->init_posterior;
   a.errors = out->errors;
   a.errors_packed = out->errors_packed;
@@ -343,7 +295,7 @@ int static_scratch(int device, unsigned char** out) {
 
 extern "C" {
 
-const char* rbp_last_error(void) { return g_err.c_str(); }
+const char* rbp_last_error(void) { return rbph::err_slot().c_str(); }
 
 const char* rbp_version(void) { return "relaybp-b200 0.2 (sm_100a)"; }
 
@@ -612,6 +564,7 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.gamma_pre = in->gamma_pre;
     a.gamma_legs_shot = in->gamma_legs_shot;
     a.n_shot_legs = in->n_shot_legs;
+    a.shot_leg_rows = in->shot_leg_rows > 0 ? in->shot_leg_rows : std::max(1, in->n_shot_legs);
     a.init_post = in->init_posterior;
     a.errors = out->errors;
     a.errors_packed = out->errors_packed;

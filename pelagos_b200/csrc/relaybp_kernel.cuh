@@ -172,8 +172,9 @@ struct DevArgs {
   const uint8_t* syn;            // [B, C]
   const float* llr_shot;         // [B, V] or null
   const float* gamma_pre;        // [B, V] or null
-  const float* gamma_legs_shot;  // [B, n_shot_legs, V] or null
+  const float* gamma_legs_shot;  // [B, shot_leg_rows, V] or null
   int n_shot_legs;
+  int shot_leg_rows;             // >= 1; leg l uses row min(l, shot_leg_rows - 1)
   const float* init_post;        // [B, V] or null
   // outputs
   uint8_t* errors;
@@ -476,7 +477,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         sought = found + 1;
         max_iter = a.set_max_iter;
         grow = (a.gamma_legs_shot && phase < a.n_shot_legs)
-                   ? a.gamma_legs_shot + (b * (long long)a.n_shot_legs + phase) * V
+                   ? a.gamma_legs_shot + (b * (long long)a.shot_leg_rows + min(phase, a.shot_leg_rows - 1)) * V
                    : a.gamma_legs + (long long)phase * V;
       }
 

@@ -500,16 +500,20 @@ class RelayBPDecoder:
     def decode_phases(self, syndromes: torch.Tensor, *, resume: Optional[torch.Tensor] = None,
                       suspend: Optional[torch.Tensor] = None, legs_begin: int = 0, legs_end: int = 0,
                       skip_relay_legs: bool = False, leg_gammas: Optional[torch.Tensor] = None,
+                      leg_gammas_legs: Optional[int] = None,
                       return_last_posterior: bool = False) -> Dict[str, torch.Tensor]:
         """Run part of a decode: from the pre-iterations (or, with `resume`, from relay leg
         `legs_begin` of the saved state) up to relay leg `legs_end` (0: all), saving the state in
-        `suspend`.  Outputs reflect the shots' state after the last phase run."""
+        `suspend`.  Outputs reflect the shots' state after the last phase run.  `leg_gammas`
+        ([B, R, V]) gives each shot its own strengths for the first `leg_gammas_legs` legs (default
+        R); leg l uses row min(l, R - 1)."""
         if self.num_gpus != 1:
             raise ValueError("resumable decoding runs on one GPU")
         if resume is not None and not 0 <= legs_begin <= self.num_sets:
             raise ValueError("legs_begin out of range")
         return self._decode_on(self.device_ids[0], syndromes, 0, self.pre_iter, None, None, skip_relay_legs,
-                               return_last_posterior, None, leg_gammas, resume, suspend, legs_begin, legs_end)
+                               return_last_posterior, None, leg_gammas, resume, suspend, legs_begin, legs_end,
+                               leg_gammas_legs)
 
     def _decode_leg_synchronous(self, syndromes, pre, init_posterior, init_gamma, return_last_posterior,
                                 prior_llr, leg_gammas):
@@ -535,7 +539,7 @@ class RelayBPDecoder:
 
     def _decode_on(self, gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
                    return_last_posterior, prior_llr, leg_gammas, resume=None, suspend=None, legs_begin=0,
-                   legs_end=0) -> Dict[str, torch.Tensor]:
+                   legs_end=0, leg_gammas_legs=None) -> Dict[str, torch.Tensor]:
         B = int(syndromes.shape[0])
         dev = self._device_strs[gpu_id]
         with torch.cuda.device(gpu_id):
@@ -550,17 +554,20 @@ class RelayBPDecoder:
                 else:
                     gamma0 = float(np.float32(self.gamma0))
             pl = prior_llr.to(**f32).contiguous() if prior_llr is not None else None
-            shot_legs, n_shot_legs = None, 0
+            shot_legs, n_shot_legs, shot_rows = None, 0, 0
             if self.gamma_draw == "per_row" and self._explicit_gammas is None and self.num_sets > 0:
                 # each device draws rows 0..B_i-1, as the reference's per-GPU loop does
                 shot_legs = self._per_row_legs(B, gpu_id, 0)
                 n_shot_legs = self.num_sets
             if leg_gammas is not None:
                 lg = leg_gammas.to(**f32).contiguous()
+                R = int(lg.shape[1])
+                L = min(R if leg_gammas_legs is None else int(leg_gammas_legs), self.num_sets)
                 if shot_legs is not None:
-                    shot_legs[:, :lg.shape[1]] = lg[:, :self.num_sets]
+                    for leg in range(L):
+                        shot_legs[:, leg] = lg[:, min(leg, R - 1)]
                 else:
-                    shot_legs, n_shot_legs = lg, min(int(lg.shape[1]), self.num_sets)
+                    shot_legs, n_shot_legs, shot_rows = lg, L, R
             W = (self.V + 31) // 32
             found = torch.empty(B, dtype=torch.int32, device=dev)
             iters = torch.empty(B, dtype=torch.int32, device=dev)
@@ -576,7 +583,7 @@ class RelayBPDecoder:
                                  n_shot_legs=n_shot_legs, pre_iter=pre,
                                  skip_relay_legs=1 if skip_relay_legs else 0,
                                  resume_state=_ptr(resume), suspend_state=_ptr(suspend),
-                                 legs_begin=int(legs_begin), legs_end=int(legs_end))
+                                 legs_begin=int(legs_begin), legs_end=int(legs_end), shot_leg_rows=shot_rows)
             outs = nat.RbpOutputs(errors=_ptr(errors), errors_packed=_ptr(packed), weights=None,
                                   weight_fixed=_ptr(wfix), found_count=_ptr(found), iterations=_ptr(iters),
                                   last_posterior=_ptr(last_post))
