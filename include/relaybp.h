@@ -244,6 +244,58 @@ RBP_API int rbp_decode_static(int32_t C, int32_t V, int32_t E,
                               const float* alpha, int32_t n_alpha, int32_t device,
                               int64_t B, const rbp_batch* in, const rbp_outputs* out, void* stream);
 
+/*
+ * Learned relay-leg proposal (no counterpart in the reference).
+ *
+ * A 2-layer edge-conditioned message-passing network on the Tanner graph
+ * (node width 64, message width 16, bf16 weights, fp32 sums) that reads a
+ * shot's syndrome and its posterior after the pre-iterations and proposes
+ * per-variable memory strengths for the first relay legs.  The strengths are
+ * handed to rbp_decode as rbp_batch.gamma_legs_shot, the per-shot form of the
+ * reference's explicit_gammas rows (src/pelagos/decoder.py:338-340, 481-491,
+ * 3685-3688), inside gamma_dist_interval (src/pelagos/utils.py:128-160).
+ * Every decoded error still has to satisfy H e = s and is still ranked by the
+ * decoder's weight rule; later legs keep the seeded table.
+ *
+ * The network owns its parameters (fp32 master copy, bf16 working copy, AdamW
+ * moments) and a training workspace sized for the largest batch seen.
+ */
+typedef struct rbp_net rbp_net;
+
+typedef struct {
+  float lr;            /* AdamW step size; 0 computes the loss and gradients only */
+  float beta1, beta2, eps, weight_decay;
+  float w_neg;         /* loss weight of variables whose pre-iteration decision is wrong */
+} rbp_net_hparams;
+
+/* Number of network parameters (the length of the flat parameter vector). */
+RBP_API int rbp_net_param_count(int64_t* n);
+
+/* Network on graph g's device; llr is the host [V] prior LLR vector.  Parameters start at 0. */
+RBP_API int rbp_net_create(const rbp_graph* g, const float* llr, rbp_net** out);
+RBP_API int rbp_net_destroy(rbp_net* n);
+
+/* Copy the flat fp32 parameters in (device pointer; resets the AdamW state) or out. */
+RBP_API int rbp_net_set_params(rbp_net* n, const float* theta, void* stream);
+RBP_API int rbp_net_get_params(const rbp_net* n, float* theta, void* stream);
+
+/* Training-path forward: logits r [B, V] (device).  syn [B, C] uint8, post [B, V] f32. */
+RBP_API int rbp_net_forward(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float* logits,
+                            void* stream);
+
+/* One training step on B shots: forward, the weighted logistic loss against
+ * target [B, V] (1 where the pre-iteration hard decision equals the true error),
+ * backward, and (lr > 0) an AdamW update.  loss (device [1]) and grads (device
+ * [n]) receive the loss and the gradient when not NULL. */
+RBP_API int rbp_net_train_step(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, const uint8_t* target,
+                               const rbp_net_hparams* hp, float* loss, float* grads, void* stream);
+
+/* Inference on the tensor cores: gammas [B, V] = lo + (hi - lo) sigmoid(r) and/or
+ * logits [B, V].  Needs a graph below 65536 edges whose per-shot state fits in
+ * one block's shared memory (RBP_ERR_UNSUPPORTED otherwise). */
+RBP_API int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float lo, float hi,
+                            float* gammas, float* logits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,14 @@ EXPORTED_SYMBOLS = (
     "rbp_mixed_capture",
     "rbp_mixed_replay",
     "rbp_mixed_query",
+    "rbp_net_param_count",
+    "rbp_net_create",
+    "rbp_net_destroy",
+    "rbp_net_set_params",
+    "rbp_net_get_params",
+    "rbp_net_forward",
+    "rbp_net_train_step",
+    "rbp_net_propose",
 )
 
 #: Bytes of the static scratch array rbp_decode_static uses (RBP_STATIC_SCRATCH_BYTES).
@@ -161,6 +169,21 @@ def _declare(lib):
     lib.rbp_mixed_replay.argtypes = [P, P]
     lib.rbp_mixed_query.restype = ct.c_int
     lib.rbp_mixed_query.argtypes = [P, i32, i32p, i32p, i32p, i32p]
+    lib.rbp_net_param_count.restype = ct.c_int
+    lib.rbp_net_param_count.argtypes = [ct.POINTER(i64)]
+    lib.rbp_net_create.restype = ct.c_int
+    lib.rbp_net_create.argtypes = [P, f32p, ct.POINTER(P)]
+    lib.rbp_net_destroy.restype = ct.c_int
+    lib.rbp_net_destroy.argtypes = [P]
+    for f in (lib.rbp_net_set_params, lib.rbp_net_get_params):
+        f.restype = ct.c_int
+        f.argtypes = [P, P, P]
+    lib.rbp_net_forward.restype = ct.c_int
+    lib.rbp_net_forward.argtypes = [P, i64, P, P, P, P]
+    lib.rbp_net_train_step.restype = ct.c_int
+    lib.rbp_net_train_step.argtypes = [P, i64, P, P, P, ct.POINTER(RbpNetHparams), P, P, P]
+    lib.rbp_net_propose.restype = ct.c_int
+    lib.rbp_net_propose.argtypes = [P, i64, P, P, ct.c_float, ct.c_float, P, P, P]
     return lib
 
 

@@ -1,0 +1,417 @@
+"""Learned relay-leg proposal: network, training on decoder-generated tuples, and
+the learned decode (pre-iterations -> network -> relay legs).
+
+The network (2-layer edge-conditioned message passing on the Tanner graph,
+node width 64, message width 16, bf16 weights, fp32 sums) reads a shot's
+syndrome and its posterior after the pre-iterations and proposes one memory
+strength per variable for the first ``learned_legs`` relay legs.  Later legs
+keep the decoder's seeded table, every decoded error must still satisfy
+H e = s, and solutions are still ranked by the decoder's weight rule, so the
+seeded legs remain the fallback.  The strengths reach the decoder as per-shot
+leg gammas, the per-shot form of the reference's ``explicit_gammas`` rows
+(src/pelagos/decoder.py:338-340, 481-491, 3685-3688), inside
+``gamma_dist_interval``.
+
+Training tuples come from the decoder itself.  For each seeded shot
+(errors e ~ Bernoulli(priors), s = H e), the decoder runs the pre-iterations
+and returns the posterior P; the target for variable v is y_v = [hard_v == e_v]
+(the pre-iteration decision agrees with the true error), i.e. the converged-leg
+strength hi where the carried posterior should be kept and lo where it should
+be overruled.  The loss is the logistic loss of sigmoid(r_v) against y_v, with
+weight ``w_neg`` on the (rare) variables whose decision is wrong.  Forward,
+backward and AdamW run in the library's own CUDA kernels (rbp_net_*).
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import json
+import time
+from dataclasses import asdict, dataclass
+from pathlib import Path
+from typing import Dict, Optional
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .decoder import RelayBPDecoder, _ptr
+
+DATA_DIR = Path(__file__).resolve().parent / "data"
+
+RELAY = dict(pre_iter=80, num_sets=100, set_max_iter=60, gamma0=0.65, gamma_dist_interval=(-0.24, 0.66),
+             stop_nconv=5, algo="relay", seed=1234)
+
+
+def param_count() -> int:
+    n = ct.c_int64()
+    nat.check(nat.lib().rbp_net_param_count(ct.byref(n)), "rbp_net_param_count")
+    return int(n.value)
+
+
+@dataclass
+class TrainConfig:
+    tuples: int = 1 << 22          # decoder-generated training tuples in total
+    batch: int = 1024              # shots per step
+    lr: float = 3e-3
+    lr_final: float = 3e-4         # cosine decay to this
+    beta1: float = 0.9
+    beta2: float = 0.999
+    eps: float = 1e-8
+    weight_decay: float = 1e-4
+    w_neg: float = 20.0
+    seed: int = 2024
+    init_seed: int = 0
+    log_every: int = 256
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """Deterministic starting point (the same as the CPU specification's)."""
+    rng = np.random.default_rng(seed)
+    H, D, T, XC = 64, 16, 4, 6
+    parts = [rng.normal(0, 1 / np.sqrt(XC), (H, XC))]
+    for _ in (1, 2):
+        parts += [rng.normal(0, 1 / np.sqrt(H), (D, H)), np.ones((T, D)) * 0.25,
+                  rng.normal(0, 0.5 / np.sqrt(D), (H, D)), np.zeros(H)]
+    parts += [rng.normal(0, 1 / np.sqrt(H), H) * 0.1, np.array([2.0, -2.0, -1.0, 0.0]), np.array([2.0])]
+    out = np.concatenate([p.reshape(-1) for p in parts]).astype(np.float32)
+    assert out.size == 4805
+    return out
+
+
+def load_params(path) -> tuple[np.ndarray, dict]:
+    z = np.load(path, allow_pickle=False)
+    return z["params"].astype(np.float32), json.loads(str(z["meta"]))
+
+
+class ProposalNet:
+    """Parameters and kernels of the proposal network on a decoder's graph and device."""
+
+    def __init__(self, decoder: RelayBPDecoder, params=None):
+        if decoder.num_gpus != 1:
+            raise ValueError("the proposal network runs on one GPU")
+        if decoder.dtype_str == "float64":
+            raise ValueError("the proposal network reads float32 posteriors (float32/16-bit message decoders)")
+        self.decoder = decoder
+        gid = decoder.device_ids[0]
+        self.device = torch.device(f"cuda:{gid}")
+        self.n_params = param_count()
+        self._h = ct.c_void_p()
+        llr = np.ascontiguousarray(decoder.log_prior_ratios, dtype=np.float32)
+        nat.check(nat.lib().rbp_net_create(decoder._native[gid]._graph, nat.f32_ptr(llr), ct.byref(self._h)),
+                  "rbp_net_create")
+        self.set_params(init_params(0) if params is None else params)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                nat.lib().rbp_net_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self._h = ct.c_void_p()
+
+    def _stream(self) -> ct.c_void_p:
+        return ct.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def set_params(self, params) -> None:
+        t = params if isinstance(params, torch.Tensor) else torch.from_numpy(np.asarray(params, np.float32))
+        t = t.to(device=self.device, dtype=torch.float32).contiguous()
+        if t.numel() != self.n_params:
+            raise ValueError(f"expected {self.n_params} parameters, got {t.numel()}")
+        nat.check(nat.lib().rbp_net_set_params(self._h, _ptr(t), self._stream()), "rbp_net_set_params")
+        torch.cuda.current_stream(self.device).synchronize()
+
+    def params(self) -> torch.Tensor:
+        out = torch.empty(self.n_params, dtype=torch.float32, device=self.device)
+        nat.check(nat.lib().rbp_net_get_params(self._h, _ptr(out), self._stream()), "rbp_net_get_params")
+        return out
+
+    def _inputs(self, syn, post):
+        syn = syn.to(device=self.device, dtype=torch.uint8).contiguous()
+        post = post.to(device=self.device, dtype=torch.float32).contiguous()
+        if syn.ndim != 2 or syn.shape[1] != self.decoder.C or tuple(post.shape) != (syn.shape[0], self.decoder.V):
+            raise ValueError("syndromes must be [B, C] and posteriors [B, V]")
+        return syn, post
+
+    def forward(self, syn: torch.Tensor, post: torch.Tensor) -> torch.Tensor:
+        """Logits [B, V] from the training-path kernels (fp32 activations)."""
+        syn, post = self._inputs(syn, post)
+        out = torch.empty(syn.shape[0], self.decoder.V, dtype=torch.float32, device=self.device)
+        nat.check(nat.lib().rbp_net_forward(self._h, syn.shape[0], _ptr(syn), _ptr(post), _ptr(out),
+                                            self._stream()), "rbp_net_forward")
+        return out
+
+    def propose(self, syn: torch.Tensor, post: torch.Tensor, lo: float, hi: float, logits: bool = False):
+        """Per-variable strengths [B, V] in (lo, hi) from the tensor-core inference kernel
+        (and the logits when ``logits``)."""
+        syn, post = self._inputs(syn, post)
+        B = syn.shape[0]
+        g = torch.empty(B, self.decoder.V, dtype=torch.float32, device=self.device)
+        r = torch.empty_like(g) if logits else None
+        nat.check(nat.lib().rbp_net_propose(self._h, B, _ptr(syn), _ptr(post), float(lo), float(hi), _ptr(g),
+                                            _ptr(r), self._stream()), "rbp_net_propose")
+        return (g, r) if logits else g
+
+    def propose_into(self, B: int, syn: torch.Tensor, post: torch.Tensor, lo: float, hi: float,
+                     gammas: torch.Tensor) -> None:
+        """propose() into caller-owned device buffers (no reshaping, no allocation)."""
+        nat.check(nat.lib().rbp_net_propose(self._h, B, _ptr(syn), _ptr(post), float(lo), float(hi), _ptr(gammas),
+                                            None, self._stream()), "rbp_net_propose")
+
+    def train_step(self, syn, post, target, cfg: TrainConfig, lr: float, loss_out: Optional[torch.Tensor] = None,
+                   grads_out: Optional[torch.Tensor] = None) -> None:
+        syn, post = self._inputs(syn, post)
+        target = target.to(device=self.device, dtype=torch.uint8).contiguous()
+        hp = nat.RbpNetHparams(lr=lr, beta1=cfg.beta1, beta2=cfg.beta2, eps=cfg.eps, weight_decay=cfg.weight_decay,
+                               w_neg=cfg.w_neg)
+        nat.check(nat.lib().rbp_net_train_step(self._h, syn.shape[0], _ptr(syn), _ptr(post), _ptr(target),
+                                               ct.byref(hp), _ptr(loss_out), _ptr(grads_out), self._stream()),
+                  "rbp_net_train_step")
+
+    def save(self, path, meta: Optional[dict] = None) -> None:
+        np.savez(path, params=self.params().cpu().numpy(), meta=json.dumps(meta or {}))
+
+
+# ---------------------------------------------------------------------------- data generation
+
+
+class ShotSampler:
+    """Seeded shots on the device: e ~ Bernoulli(priors), s = H e mod 2."""
+
+    def __init__(self, H_csr, priors, device, seed: int):
+        self.device = torch.device(device)
+        Hc = H_csr.tocsr()
+        self.C, self.V = Hc.shape
+        self.HT = torch.from_numpy(Hc.toarray().T.astype(np.float32)).to(self.device)  # [V, C]
+        self.p = torch.from_numpy(np.asarray(priors, np.float32)).to(self.device)
+        self.gen = torch.Generator(device=self.device)
+        self.gen.manual_seed(seed)
+
+    def sample(self, B: int):
+        e = (torch.rand(B, self.V, generator=self.gen, device=self.device) < self.p).to(torch.uint8)
+        s = torch.remainder(e.float() @ self.HT, 2).to(torch.uint8)
+        return e, s
+
+
+def make_tuples(decoder: RelayBPDecoder, syn: torch.Tensor, err: torch.Tensor):
+    """(posterior after the pre-iterations, target [hard == e]) for each shot."""
+    pre = decoder.decode_phases(syn, skip_relay_legs=True, return_last_posterior=True)
+    post = pre["last_posterior"].float()
+    target = ((post <= 0).to(torch.uint8) == err).to(torch.uint8)
+    return post, target
+
+
+def train(decoder: RelayBPDecoder, H_csr, priors, cfg: TrainConfig, net: Optional[ProposalNet] = None,
+          log=print) -> tuple[ProposalNet, list]:
+    """Train on cfg.tuples decoder-generated tuples; returns the network and the loss log."""
+    net = net or ProposalNet(decoder, init_params(cfg.init_seed))
+    sampler = ShotSampler(H_csr, priors, net.device, cfg.seed)
+    steps = max(1, cfg.tuples // cfg.batch)
+    loss = torch.zeros(1, device=net.device)
+    hist, acc, t0 = [], torch.zeros(1, device=net.device), time.time()
+    for step in range(steps):
+        err, syn = sampler.sample(cfg.batch)
+        post, target = make_tuples(decoder, syn, err)
+        lr = cfg.lr_final + 0.5 * (cfg.lr - cfg.lr_final) * (1 + np.cos(np.pi * step / steps))
+        net.train_step(syn, post, target, cfg, lr, loss_out=loss)
+        acc += loss
+        if (step + 1) % cfg.log_every == 0 or step + 1 == steps:
+            k = (step % cfg.log_every) + 1
+            mean = float(acc) / k
+            acc.zero_()
+            hist.append({"step": step + 1, "tuples": (step + 1) * cfg.batch, "loss": mean,
+                         "seconds": time.time() - t0})
+            log(json.dumps(hist[-1]))
+    return net, hist
+
+
+# ---------------------------------------------------------------------------- learned decode
+
+
+class LearnedRelayBPDecoder:
+    """Relay-BP with learned strengths for the first relay legs.
+
+    ``decode(syndromes)`` runs three launches on the current stream: the
+    pre-iterations (saving each shot's state and posterior), the network's
+    tensor-core inference, and the relay legs resumed from the saved state with
+    the proposed strengths on legs 0..learned_legs-1 and the seeded table after.
+    Outputs have the same keys as ``RelayBPDecoder.decode``.
+    """
+
+    def __init__(self, decoder: RelayBPDecoder, net: ProposalNet, learned_legs: int = 4):
+        if decoder.algo != "relay":
+            raise ValueError("learned legs need algo='relay'")
+        if decoder.num_gpus != 1:
+            raise ValueError("the learned decode runs on one GPU")
+        self.dec, self.net = decoder, net
+        self.learned_legs = int(min(learned_legs, decoder.num_sets))
+        self.lo, self.hi = (float(x) for x in decoder.gamma_dist_interval)
+        self._bufs: Dict[int, dict] = {}
+
+    def _buffers(self, B: int) -> dict:
+        b = self._bufs.get(B)
+        if b is None:
+            d, dev = self.dec, self.net.device
+            b = {
+                "state": d.new_state(B),
+                "post": torch.empty(B, d.V, dtype=torch.float32, device=dev),
+                "gammas": torch.empty(B, d.V, dtype=torch.float32, device=dev),
+                "found": torch.empty(B, dtype=torch.int32, device=dev),
+                "iters": torch.empty(B, dtype=torch.int32, device=dev),
+                "wfix": torch.empty(B, dtype=torch.int64, device=dev),
+                "errors": torch.empty(B, d.V, dtype=torch.uint8, device=dev),
+            }
+            self._bufs = {B: b}  # keep one batch size
+        return b
+
+    def decode_into(self, syn: torch.Tensor) -> dict:
+        """Launch the three phases into the persistent buffers of this batch size (no host sync)."""
+        d = self.dec
+        B = int(syn.shape[0])
+        bf = self._buffers(B)
+        gid = d.device_ids[0]
+        stream = torch.cuda.current_stream(self.net.device).cuda_stream
+        gamma0 = float(np.float32(d.gamma0))
+        pre_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter, skip_relay_legs=1,
+                              suspend_state=_ptr(bf["state"]))
+        pre_out = nat.RbpOutputs(found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]),
+                                 last_posterior=_ptr(bf["post"]))
+        d._native[gid].decode(B, pre_in, pre_out, stream)
+        self.net.propose_into(B, syn, bf["post"], self.lo, self.hi, bf["gammas"])
+        legs_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter,
+                               gamma_legs_shot=_ptr(bf["gammas"]), n_shot_legs=self.learned_legs, shot_leg_rows=1,
+                               resume_state=_ptr(bf["state"]), legs_begin=0)
+        legs_out = nat.RbpOutputs(errors=_ptr(bf["errors"]), weight_fixed=_ptr(bf["wfix"]),
+                                  found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
+        d._native[gid].decode(B, legs_in, legs_out, stream)
+        return bf
+
+    def decode(self, syndromes: torch.Tensor) -> Dict[str, torch.Tensor]:
+        d = self.dec
+        syn = syndromes.to(device=self.net.device, dtype=torch.uint8).contiguous()
+        if syn.ndim != 2 or syn.shape[1] != d.C:
+            raise ValueError(f"syndromes must be [B, {d.C}]")
+        if syn.shape[0] == 0:
+            return d.decode(syn)
+        bf = self.decode_into(syn)
+        wfix, found = bf["wfix"].clone(), bf["found"].clone()
+        has = wfix != torch.iinfo(torch.int64).max
+        weights = torch.where(has, wfix.to(torch.float64) * (2.0 ** -32),
+                              torch.full_like(wfix, 0, dtype=torch.float64) + float("inf")).to(torch.float32)
+        return {
+            "errors": bf["errors"].clone(),
+            "weights": weights,
+            "valid_mask": found >= d.stop_nconv,
+            "iterations": bf["iters"].clone(),
+            "found_count": found,
+            "unconverged_indices": torch.nonzero(found < d.stop_nconv).flatten().to(torch.int32),
+            "weight_fixed": wfix,
+        }
+
+
+def default_weights_path(workload: str = "bb144_phen", p: float = 0.003) -> Path:
+    return DATA_DIR / f"proposal_{workload}_p{str(p).replace('.', '')}.npz"
+
+
+# ---------------------------------------------------------------------------- evaluation and CLI
+
+
+def _timed(fn):
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def evaluate(workload, net: ProposalNet, decoder: RelayBPDecoder, shots: int, seed: int, chunk: int = 262144,
+             learned_legs: int = 4) -> dict:
+    """Plain and learned decodes of the same fresh seeded shots: logical error rate (Wilson 95%
+    interval), mean iterations and decode time of each (device time, syndromes resident)."""
+    from .experiments import wilson
+
+    learned = LearnedRelayBPDecoder(decoder, net, learned_legs=learned_legs)
+    rows = {"plain": {"fails": 0, "unconv": 0, "iters": 0, "ms": 0.0},
+            "learned": {"fails": 0, "unconv": 0, "iters": 0, "ms": 0.0}}
+    done, k = 0, 0
+    while done < shots:
+        n = min(chunk, shots - done)
+        err, syn = workload.sample(n, seed=seed + k)
+        syn_d = torch.from_numpy(syn).to(net.device)
+        if k == 0:
+            decoder.decode(syn_d)
+            learned.decode(syn_d)
+        for name, fn in (("plain", lambda: decoder.decode(syn_d)), ("learned", lambda: learned.decode(syn_d))):
+            out, ms = _timed(fn)
+            o = {kk: v.cpu().numpy() for kk, v in out.items() if isinstance(v, torch.Tensor)}
+            conv = o["found_count"] > 0
+            f = workload.logical_failures(err, o["errors"], conv)
+            r = rows[name]
+            r["fails"] += int(f.sum())
+            r["unconv"] += int((~conv).sum())
+            r["iters"] += int(o["iterations"].astype(np.int64).sum())
+            r["ms"] += ms
+        done += n
+        k += 1
+    res = {"shots": shots, "seed": seed, "learned_legs": learned_legs}
+    for name, r in rows.items():
+        lo, hi = wilson(r["fails"], shots)
+        res[name] = {"ler": r["fails"] / shots, "ler_ci95": [lo, hi], "failures": r["fails"],
+                     "unconverged": r["unconv"], "mean_iterations": r["iters"] / shots,
+                     "decode_ms": r["ms"], "shots_per_s": shots / (r["ms"] * 1e-3)}
+    res["speedup"] = res["learned"]["shots_per_s"] / res["plain"]["shots_per_s"]
+    res["iteration_ratio"] = res["plain"]["mean_iterations"] / res["learned"]["mean_iterations"]
+    pl, le = res["plain"]["ler_ci95"], res["learned"]["ler_ci95"]
+    res["ler_intervals_overlap"] = bool(le[0] <= pl[1] and pl[0] <= le[1])
+    return res
+
+
+def main(argv=None):
+    import argparse
+
+    from . import codes
+
+    ap = argparse.ArgumentParser(prog="python -m pelagos_b200.proposal")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train", help="train on decoder-generated tuples and save the weights")
+    t.add_argument("--workload", default="bb144_phen")
+    t.add_argument("--p", type=float, default=0.003)
+    t.add_argument("--tuples", type=int, default=1 << 22)
+    t.add_argument("--batch", type=int, default=1024)
+    t.add_argument("--lr", type=float, default=3e-3)
+    t.add_argument("--w-neg", type=float, default=20.0)
+    t.add_argument("--seed", type=int, default=2024)
+    t.add_argument("--out", default=None)
+    e = sub.add_parser("eval", help="plain vs learned decode on fresh seeded shots")
+    e.add_argument("--workload", default="bb144_phen")
+    e.add_argument("--p", type=float, default=0.003)
+    e.add_argument("--weights", default=None)
+    e.add_argument("--shots", type=int, default=1 << 20)
+    e.add_argument("--seed", type=int, default=900001)
+    e.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    w = codes.workload(a.workload, p=a.p)
+    dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    if a.cmd == "train":
+        cfg = TrainConfig(tuples=a.tuples, batch=a.batch, lr=a.lr, w_neg=a.w_neg, seed=a.seed)
+        net, hist = train(dec, w.H, w.priors, cfg)
+        out = a.out or str(default_weights_path(a.workload, a.p))
+        Path(out).parent.mkdir(parents=True, exist_ok=True)
+        net.save(out, meta={"workload": a.workload, "p": a.p, "train": asdict(cfg), "log": hist[-8:],
+                            "decoder": RELAY})
+        print(json.dumps({"saved": out, "final_loss": hist[-1]["loss"], "seconds": hist[-1]["seconds"]}))
+    else:
+        params, meta = load_params(a.weights or default_weights_path(a.workload, a.p))
+        net = ProposalNet(dec, params)
+        res = evaluate(w, net, dec, a.shots, a.seed)
+        res["weights_meta"] = {k: meta.get(k) for k in ("workload", "p", "train")}
+        print(json.dumps(res, indent=1))
+        if a.out:
+            Path(a.out).write_text(json.dumps(res, indent=1))
+
+
+if __name__ == "__main__":
+    main()
