@@ -141,6 +141,11 @@ typedef struct {
   /* Rows per shot in gamma_legs_shot (0: n_shot_legs).  Leg l < n_shot_legs
    * uses row min(l, shot_leg_rows - 1), so one row can serve several legs. */
   int32_t shot_leg_rows;
+  /* Order in which the persistent kernel takes the shots (device [B], a
+   * permutation of 0..B-1), or NULL for 0, 1, ..., B-1.  Results do not depend
+   * on it; putting the shots that will run longest first keeps them from
+   * finishing after everything else.  Entries outside [0, B) are skipped. */
+  const int32_t* shot_order;
 } rbp_batch;
 
 /* Outputs (device memory).  Any may be NULL except found_count/iterations. */

@@ -97,6 +97,7 @@ class RbpBatch(ct.Structure):
         ("legs_begin", ct.c_int32),
         ("legs_end", ct.c_int32),
         ("shot_leg_rows", ct.c_int32),
+        ("shot_order", ct.c_void_p),
     ]
 
 

@@ -473,10 +473,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
   return *reinterpret_cast<const uint32_t*>(&p);
 }
 
-__device__ __forceinline__ uint32_t sw_pair(const bf16* w, int i) {  // i even
-  return *reinterpret_cast<const uint32_t*>(w + i);
-}
-
 __device__ __forceinline__ float sw_f(const bf16* w, int i) { return __bfloat162float(w[i]); }
 
 __device__ __forceinline__ void unpack8(const uint4& q, float (&f)[8]) {
@@ -498,6 +494,46 @@ __device__ __forceinline__ uint4 pack8(const float (&f)[8]) {
   return q;
 }
 
+// B operands of the tensor-core layers, stored per fragment so that a warp
+// reads each fragment as 32 consecutive words (lane l at word l): no bank
+// conflicts, unlike reading the [n][k] weight rows directly (a 128-byte row
+// stride puts the 8 rows of a fragment in one bank).
+constexpr int FR_E = 0;                   // [nt 8] (k 0..7; k >= 6 is zero)
+constexpr int FR_W1 = FR_E + 8 * 32;      // [nt 2][kk 4][half 2]
+constexpr int FR_W2 = FR_W1 + 16 * 32;
+constexpr int FR_U1 = FR_W2 + 16 * 32;    // [nt 8][half 2]
+constexpr int FR_U2 = FR_U1 + 16 * 32;
+constexpr int FR_O = FR_U2 + 16 * 32;     // [kk 4][half 2], column 0 only
+constexpr int FR_WORDS = FR_O + 8 * 32;
+
+__device__ __forceinline__ uint32_t theta_pair(const bf16* th, int i) {
+  return (uint32_t)__bfloat16_as_ushort(th[i]) | ((uint32_t)__bfloat16_as_ushort(th[i + 1]) << 16);
+}
+
+// Word w of the fragment table (lane = w % 32: row n = nt*8 + lane/4, columns k, k+1 with k = ... + 2 (lane%4)).
+__device__ uint32_t fragment_word(const bf16* th, int w) {
+  const int lane = w & 31, f = w >> 5, gq = lane >> 2, k2 = 2 * (lane & 3);
+  if (w < FR_W1) {
+    const int n = f * 8 + gq;
+    return k2 < NX ? theta_pair(th, P_E + n * NX + k2) : 0u;
+  }
+  if (w < FR_U1) {
+    const int base = w < FR_W2 ? P_W1 : P_W2;
+    const int ff = f - (w < FR_W2 ? FR_W1 : FR_W2) / 32;
+    const int nt = ff >> 3, kk = (ff >> 1) & 3, half = ff & 1;
+    return theta_pair(th, base + (nt * 8 + gq) * NH + kk * 16 + half * 8 + k2);
+  }
+  if (w < FR_O) {
+    const int base = w < FR_U2 ? P_U1 : P_U2;
+    const int ff = f - (w < FR_U2 ? FR_U1 : FR_U2) / 32;
+    const int nt = ff >> 1, half = ff & 1;
+    return theta_pair(th, base + (nt * 8 + gq) * ND + half * 8 + k2);
+  }
+  const int ff = f - FR_O / 32;
+  const int kk = ff >> 1, half = ff & 1;
+  return gq == 0 ? theta_pair(th, P_O + kk * 16 + half * 8 + k2) : 0u;
+}
+
 struct ProposeArgs {
   long long B;
   const uint8_t* syn;       // [B, C]
@@ -509,7 +545,7 @@ struct ProposeArgs {
   const float* chk_lmean;   // [C] mean of the check's variables' tanh(llr/16)
   const uint16_t* graph16;  // chk_ptr [C+1], chk_var [E], var_ptr [V+1], var_chk [E]
   int graph16_len;          // entries, a multiple of 8
-  int off_w, off_g, off_x, off_m, off_n, off_a1, off_a2, off_th, off_tu, off_syn;  // shared-memory byte offsets
+  int off_w, off_fr, off_g, off_x, off_m, off_n, off_a1, off_a2, off_th, off_tu, off_syn;  // shared-memory byte offsets
 };
 
 // Rows r0, r0+8 of a bf16 [rows][16] array as an A fragment (zero past C).
@@ -522,7 +558,7 @@ __device__ __forceinline__ void load_a16(const bf16* s, int r0, int tq, int C, u
 }
 
 // q0 = x^ E^T for the warp's 16 checks (8 n-tiles of 8 columns); x rows are 8 wide.
-__device__ __forceinline__ void tile_embed(const bf16* sw, const bf16* s_x, int r0, int gq, int tq, int C,
+__device__ __forceinline__ void tile_embed(const uint32_t* fr, const bf16* s_x, int r0, int lane, int tq, int C,
                                            float (&acc)[8][4]) {
   uint32_t a[4];
   a[0] = (r0 < C && tq < 3) ? *reinterpret_cast<const uint32_t*>(s_x + r0 * 8 + 2 * tq) : 0u;
@@ -532,8 +568,7 @@ __device__ __forceinline__ void tile_embed(const bf16* sw, const bf16* s_x, int 
 #pragma unroll
   for (int nt = 0; nt < 8; ++nt) {
     acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-    const uint32_t b0 = tq < 3 ? sw_pair(sw, P_E + (nt * 8 + gq) * NX + 2 * tq) : 0u;
-    mma_bf16(acc[nt], a, b0, 0u);
+    mma_bf16(acc[nt], a, fr[FR_E + nt * 32 + lane], 0u);
   }
 }
 
@@ -549,16 +584,16 @@ __device__ __forceinline__ void relu_to_a(const float (&acc)[8][4], uint32_t (&g
 }
 
 // m = round(g^ W^T) for the tile, stored as bf16 rows of 16.
-__device__ __forceinline__ void tile_message(const bf16* sw, int pw, const uint32_t (&ga)[4][4], int r0, int gq,
-                                             int tq, int C, bf16* s_m) {
+__device__ __forceinline__ void tile_message(const uint32_t* fr, int fw, const uint32_t (&ga)[4][4], int r0,
+                                             int lane, int tq, int C, bf16* s_m) {
   float mc[2][4];
 #pragma unroll
   for (int nt = 0; nt < 2; ++nt) {
     mc[nt][0] = mc[nt][1] = mc[nt][2] = mc[nt][3] = 0.f;
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
-      const int base = pw + (nt * 8 + gq) * NH + kk * 16 + 2 * tq;
-      mma_bf16(mc[nt], ga[kk], sw_pair(sw, base), sw_pair(sw, base + 8));
+      const uint32_t* f = fr + fw + (nt * 8 + kk * 2) * 32 + lane;
+      mma_bf16(mc[nt], ga[kk], f[0], f[32]);
     }
   }
   const int r1 = r0 + 8;
@@ -570,8 +605,8 @@ __device__ __forceinline__ void tile_message(const bf16* sw, int pw, const uint3
 }
 
 // acc <- relu(acc) + b + a^ U^T  (the residual update of one layer)
-__device__ __forceinline__ void tile_update(const bf16* sw, int pu, int pb, const bf16* s_a, int r0, int gq, int tq,
-                                            int C, float (&acc)[8][4]) {
+__device__ __forceinline__ void tile_update(const bf16* sw, const uint32_t* fr, int fu, int pb, const bf16* s_a,
+                                            int r0, int lane, int tq, int C, float (&acc)[8][4]) {
   uint32_t a[4];
   load_a16(s_a, r0, tq, C, a);
 #pragma unroll
@@ -582,8 +617,8 @@ __device__ __forceinline__ void tile_update(const bf16* sw, int pu, int pb, cons
     acc[nt][1] = fmaxf(acc[nt][1], 0.f) + bb.y;
     acc[nt][2] = fmaxf(acc[nt][2], 0.f) + bb.x;
     acc[nt][3] = fmaxf(acc[nt][3], 0.f) + bb.y;
-    const int base = pu + (nt * 8 + gq) * ND + 2 * tq;
-    mma_bf16(acc[nt], a, sw_pair(sw, base), sw_pair(sw, base + 8));
+    const uint32_t* f = fr + fu + nt * 64 + lane;
+    mma_bf16(acc[nt], a, f[0], f[32]);
   }
 }
 
@@ -592,6 +627,7 @@ constexpr int PROPOSE_THREADS = 512;
 __global__ void __launch_bounds__(PROPOSE_THREADS, 1) net_propose_kernel(NetGraph g, ProposeArgs pa) {
   extern __shared__ __align__(16) unsigned char smem[];
   bf16* sw = reinterpret_cast<bf16*>(smem + pa.off_w);
+  uint32_t* fr = reinterpret_cast<uint32_t*>(smem + pa.off_fr);
   bf16* s_x = reinterpret_cast<bf16*>(smem + pa.off_x);
   bf16* s_m = reinterpret_cast<bf16*>(smem + pa.off_m);
   float* s_o = reinterpret_cast<float*>(smem + pa.off_m);  // reuses the message rows after layer 2
@@ -612,6 +648,7 @@ __global__ void __launch_bounds__(PROPOSE_THREADS, 1) net_propose_kernel(NetGrap
   const uint16_t* var_chk = var_ptr + V + 1;
 
   for (int i = tid; i < N_PARAMS; i += blockDim.x) sw[i] = pa.theta[i];
+  for (int i = tid; i < FR_WORDS; i += blockDim.x) fr[i] = fragment_word(pa.theta, i);
   for (int i = tid; i < pa.graph16_len / 8; i += blockDim.x)
     reinterpret_cast<uint4*>(sg)[i] = __ldg(reinterpret_cast<const uint4*>(pa.graph16) + i);
   __syncthreads();
@@ -657,10 +694,10 @@ __global__ void __launch_bounds__(PROPOSE_THREADS, 1) net_propose_kernel(NetGrap
         float acc[8][4];
         uint32_t ga[4][4];
         const int r0 = tile * 16 + gq;
-        tile_embed(sw, s_x, r0, gq, tq, C, acc);
-        if (layer == 2) tile_update(sw, P_U1, P_B1, s_a1, r0, gq, tq, C, acc);
+        tile_embed(fr, s_x, r0, lane, tq, C, acc);
+        if (layer == 2) tile_update(sw, fr, FR_U1, P_B1, s_a1, r0, lane, tq, C, acc);
         relu_to_a(acc, ga);
-        tile_message(sw, layer == 1 ? P_W1 : P_W2, ga, r0, gq, tq, C, s_m);
+        tile_message(fr, layer == 1 ? FR_W1 : FR_W2, ga, r0, lane, tq, C, s_m);
       }
       __syncthreads();
       // per half h of the 16 channels: n_v = round(sum_{c in M(v)} m_c), then
@@ -699,17 +736,13 @@ __global__ void __launch_bounds__(PROPOSE_THREADS, 1) net_propose_kernel(NetGrap
       float acc[8][4];
       uint32_t ga[4][4];
       const int r0 = tile * 16 + gq;
-      tile_embed(sw, s_x, r0, gq, tq, C, acc);
-      tile_update(sw, P_U1, P_B1, s_a1, r0, gq, tq, C, acc);
-      tile_update(sw, P_U2, P_B2, s_a2, r0, gq, tq, C, acc);
+      tile_embed(fr, s_x, r0, lane, tq, C, acc);
+      tile_update(sw, fr, FR_U1, P_B1, s_a1, r0, lane, tq, C, acc);
+      tile_update(sw, fr, FR_U2, P_B2, s_a2, r0, lane, tq, C, acc);
       relu_to_a(acc, ga);
       float oc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const uint32_t b0 = gq == 0 ? sw_pair(sw, P_O + kk * 16 + 2 * tq) : 0u;
-        const uint32_t b1 = gq == 0 ? sw_pair(sw, P_O + kk * 16 + 8 + 2 * tq) : 0u;
-        mma_bf16(oc, ga[kk], b0, b1);
-      }
+      for (int kk = 0; kk < 4; ++kk) mma_bf16(oc, ga[kk], fr[FR_O + kk * 64 + lane], fr[FR_O + kk * 64 + 32 + lane]);
       if (tq == 0) {
         if (r0 < C) s_o[r0] = oc[0];
         if (r0 + 8 < C) s_o[r0 + 8] = oc[2];
@@ -902,6 +935,7 @@ int rbp_net_create(const rbp_graph* g, const float* llr, rbp_net** out) {
   const int g16 = (2 * C + 2 * V + 2 + 2 * E + 7) / 8 * 8;
   n->layout.graph16_len = g16;
   n->layout.off_w = take(N_PARAMS * 2);
+  n->layout.off_fr = take(FR_WORDS * 4);
   n->layout.off_g = take(g16 * 2);
   n->layout.off_x = take(C * 8 * 2);
   n->layout.off_m = take(std::max(C * ND * 2, C * 4));

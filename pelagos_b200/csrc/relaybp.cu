@@ -235,6 +235,7 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.gamma_legs_shot = in->gamma_legs_shot;
   a.n_shot_legs = in->n_shot_legs;
   a.shot_leg_rows = in->shot_leg_rows > 0 ? in->shot_leg_rows : std::max(1, in->n_shot_legs);
+  a.order = in->shot_order;
   a.init_post = in->init_posterior;
   a.errors = out->errors;
   a.errors_packed = out->errors_packed;
@@ -565,6 +566,7 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.gamma_legs_shot = in->gamma_legs_shot;
     a.n_shot_legs = in->n_shot_legs;
     a.shot_leg_rows = in->shot_leg_rows > 0 ? in->shot_leg_rows : std::max(1, in->n_shot_legs);
+    a.order = in->shot_order;
     a.init_post = in->init_posterior;
     a.errors = out->errors;
     a.errors_packed = out->errors_packed;

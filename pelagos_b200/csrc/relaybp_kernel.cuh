@@ -192,6 +192,7 @@ struct DevArgs {
   int state_stride;
   // scheduling
   int* queue;
+  const int* order;              // [B] queue position -> shot index, or null (identity)
   int group_threads, groups;
   // shared-memory layout (byte offsets)
   int off_chk_deg, off_llr, off_group0, group_bytes;
@@ -407,10 +408,22 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
   A gam[VPT];
 
   while (true) {
-    if (t == 0) *shot_slot = (long long)atomicAdd(a.queue, 1);
+    if (t == 0) {
+      const long long q = (long long)atomicAdd(a.queue, 1);
+      long long sb = q;
+      if (q < a.B && a.order) {
+        sb = (long long)a.order[q];
+        if (sb < 0 || sb >= a.B) sb = -1;  // not a shot index: this queue entry is skipped
+      }
+      *shot_slot = sb;
+    }
     group_sync(bar, G);
     const long long b = *shot_slot;
     if (b >= a.B) break;
+    if (b < 0) {
+      group_sync(bar, G);  // every thread has read the slot before thread 0 refills it
+      continue;
+    }
 
     // ---------------- per-shot setup (decoder.py:3429-3478)
     const uint8_t* syn_row = a.syn + b * (long long)C;

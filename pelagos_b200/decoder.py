@@ -67,6 +67,9 @@ def _ptr(t: Optional[torch.Tensor]):
     return ct.c_void_p(t.data_ptr()) if t is not None else ct.c_void_p(0)
 
 
+#: Batches at least this large decode with the unconverged shots queued first (hard_shots_first).
+HARD_FIRST_MIN_BATCH = 1024
+
 class _NativeDecoder:
     """Owns one device's rbp_graph + rbp_decoder handles."""
 
@@ -135,6 +138,12 @@ class RelayBPDecoder:
     * ``mix_rounding``: rounding of the memory mix (1-g)*llr + g*posterior:
       "separate" (default; one rounding per operation), "fma_gp" or "fma_lp";
     * ``launch``: optional (group_threads, groups_per_block) kernel shape.
+    * ``hard_shots_first`` (default True): a relay decode of at least 1024 shots
+      runs as two launches, the pre-iterations and then the relay legs resumed
+      from each shot's saved state, with the shots the pre-iterations left
+      unconverged queued first.  Those few shots run up to
+      pre_iter + num_sets * set_max_iter iterations; started first, they finish
+      alongside the bulk instead of after it.  Results are identical.
     """
 
     def __init__(
@@ -170,6 +179,7 @@ class RelayBPDecoder:
         *,
         mix_rounding: str = "separate",
         launch: Optional[Tuple[int, int]] = None,
+        hard_shots_first: bool = True,
     ):
         if unconverged_correction not in UNCONVERGED_CORRECTIONS:
             raise ValueError(
@@ -267,6 +277,7 @@ class RelayBPDecoder:
         torch.manual_seed(seed)
 
         self._launch = tuple(launch) if launch is not None else None
+        self.hard_shots_first = bool(hard_shots_first)
         self._native: Dict[int, _NativeDecoder] = {}
         self._legs_broadcast: Dict[int, torch.Tensor] = {}
         self._alpha_len = max(self.pre_iter, self.set_max_iter, 1)
@@ -457,14 +468,21 @@ class RelayBPDecoder:
             if self.fast_max_unconverged_pct is not None and not skip_relay_legs:
                 return self._decode_leg_synchronous(syndromes, pre, init_posterior, init_gamma,
                                                     return_last_posterior, prior_llr, leg_gammas)
+            if (self.hard_shots_first and not skip_relay_legs and self.num_sets > 0 and pre > 0
+                    and B >= HARD_FIRST_MIN_BATCH):
+                return self._decode_hard_first(self.device_ids[0], syndromes, pre, init_posterior, init_gamma,
+                                               return_last_posterior, prior_llr, leg_gammas)
             return self._decode_on(self.device_ids[0], syndromes, 0, pre, init_posterior, init_gamma,
                                    skip_relay_legs, return_last_posterior, prior_llr, leg_gammas)
         splits = self._split_batch(B, self.num_gpus)
         parts = []
         for gpu_id, (s0, s1) in zip(self.device_ids, splits):
             lg = leg_gammas[s0:s1] if leg_gammas is not None else None
-            parts.append(self._decode_on(gpu_id, syndromes[s0:s1], s0, pre, None, None, False, False,
-                                         None, lg))
+            if self.hard_shots_first and self.num_sets > 0 and pre > 0 and s1 - s0 >= HARD_FIRST_MIN_BATCH:
+                parts.append(self._decode_hard_first(gpu_id, syndromes[s0:s1], pre, None, None, False, None, lg))
+            else:
+                parts.append(self._decode_on(gpu_id, syndromes[s0:s1], s0, pre, None, None, False, False,
+                                             None, lg))
         return self._gather(parts, splits)
 
     @staticmethod
@@ -487,10 +505,11 @@ class RelayBPDecoder:
         out["unconverged_indices"] = torch.cat(unc, 0).to(torch.int32)
         return out
 
-    def state_bytes(self) -> int:
+    def state_bytes(self, gpu_id: Optional[int] = None) -> int:
         """Bytes of one shot's saved decode state (resumable decoding)."""
         b = ct.c_int64()
-        nat.check(nat.lib().rbp_state_bytes(self._native[self.device_ids[0]]._dec, ct.byref(b)), "rbp_state_bytes")
+        gid = self.device_ids[0] if gpu_id is None else gpu_id
+        nat.check(nat.lib().rbp_state_bytes(self._native[gid]._dec, ct.byref(b)), "rbp_state_bytes")
         return int(b.value)
 
     def new_state(self, B: int) -> torch.Tensor:
@@ -537,9 +556,37 @@ class RelayBPDecoder:
                 break
         return out
 
+    def _state_buffer(self, gpu_id: int, B: int) -> torch.Tensor:
+        """Per-device saved-state buffer of the two-launch decode, kept for the next call of the same
+        or a smaller batch (a fresh 11 KB-per-shot allocation per call stalls the allocator)."""
+        cache = self.__dict__.setdefault("_state_cache", {})
+        buf = cache.get(gpu_id)
+        if buf is None or buf.shape[0] < B:
+            cache[gpu_id] = None
+            buf = torch.empty(B, self.state_bytes(gpu_id), dtype=torch.uint8, device=self._device_strs[gpu_id])
+            cache[gpu_id] = buf
+        return buf[:B]
+
+    def _decode_hard_first(self, gpu_id, syndromes, pre, init_posterior, init_gamma, return_last_posterior,
+                           prior_llr, leg_gammas) -> Dict[str, torch.Tensor]:
+        """Pre-iterations, then the relay legs with the unconverged shots queued first."""
+        B = int(syndromes.shape[0])
+        dev = self._device_strs[gpu_id]
+        with torch.cuda.device(gpu_id):
+            syn = syndromes.to(device=dev, dtype=torch.uint8).contiguous()
+            state = self._state_buffer(gpu_id, B)
+            first = self._decode_on(gpu_id, syn, 0, pre, init_posterior, init_gamma, True, False, prior_llr,
+                                    leg_gammas, None, state, 0, 0, light=True)
+            # stable: converged shots (key 1) keep their order after the unconverged ones (key 0)
+            order = torch.argsort((first["found_count"] > 0).to(torch.uint8), stable=True).to(torch.int32)
+            return self._decode_on(gpu_id, syn, 0, pre, None, None, False, return_last_posterior, prior_llr,
+                                   leg_gammas, state, None, 0, 0, order=order)
+
     def _decode_on(self, gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
                    return_last_posterior, prior_llr, leg_gammas, resume=None, suspend=None, legs_begin=0,
-                   legs_end=0, leg_gammas_legs=None) -> Dict[str, torch.Tensor]:
+                   legs_end=0, leg_gammas_legs=None, order=None, light=False) -> Dict[str, torch.Tensor]:
+        """One launch.  ``order`` sets the queue order; ``light`` returns only found_count and
+        iterations (no error rows, no host synchronisation)."""
         B = int(syndromes.shape[0])
         dev = self._device_strs[gpu_id]
         with torch.cuda.device(gpu_id):
@@ -573,7 +620,9 @@ class RelayBPDecoder:
             iters = torch.empty(B, dtype=torch.int32, device=dev)
             wfix = torch.empty(B, dtype=torch.int64, device=dev)
             errors = packed = None
-            if self.bitpack_output:
+            if light:
+                pass
+            elif self.bitpack_output:
                 packed = torch.empty(B, W, dtype=torch.int32, device=dev)
             else:
                 errors = torch.empty(B, self.V, dtype=torch.uint8, device=dev)
@@ -583,12 +632,15 @@ class RelayBPDecoder:
                                  n_shot_legs=n_shot_legs, pre_iter=pre,
                                  skip_relay_legs=1 if skip_relay_legs else 0,
                                  resume_state=_ptr(resume), suspend_state=_ptr(suspend),
-                                 legs_begin=int(legs_begin), legs_end=int(legs_end), shot_leg_rows=shot_rows)
+                                 legs_begin=int(legs_begin), legs_end=int(legs_end), shot_leg_rows=shot_rows,
+                                 shot_order=_ptr(order))
             outs = nat.RbpOutputs(errors=_ptr(errors), errors_packed=_ptr(packed), weights=None,
                                   weight_fixed=_ptr(wfix), found_count=_ptr(found), iterations=_ptr(iters),
                                   last_posterior=_ptr(last_post))
             stream = torch.cuda.current_stream(gpu_id).cuda_stream
             self._native[gpu_id].decode(B, batch, outs, stream)
+            if light:
+                return {"found_count": found, "iterations": iters}
             has = wfix != torch.iinfo(torch.int64).max
             wdt = torch.float64 if self.dtype_str == "float64" else torch.float32
             weights = torch.where(has, wfix.to(torch.float64) * (2.0 ** -32),
