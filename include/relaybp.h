@@ -296,10 +296,15 @@ RBP_API int rbp_net_train_step(rbp_net* n, int64_t B, const uint8_t* syn, const 
                                const rbp_net_hparams* hp, float* loss, float* grads, void* stream);
 
 /* Inference on the tensor cores: gammas [B, V] = lo + (hi - lo) sigmoid(r) and/or
- * logits [B, V].  Needs a graph below 65536 edges whose per-shot state fits in
- * one block's shared memory (RBP_ERR_UNSUPPORTED otherwise). */
+ * logits [B, V].  With shot_list (device [B]) only the shots shot_list[i],
+ * i < *list_count (a device int32; all B entries when list_count is NULL),
+ * are evaluated and their rows written; other rows are left as they are, so a
+ * caller can evaluate a subset chosen on the device without a host round trip.
+ * Needs a graph below 65536 edges whose per-shot state fits in one block's
+ * shared memory (RBP_ERR_UNSUPPORTED otherwise). */
 RBP_API int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float lo, float hi,
-                            float* gammas, float* logits, void* stream);
+                            const int32_t* shot_list, const int32_t* list_count, float* gammas, float* logits,
+                            void* stream);
 
 #ifdef __cplusplus
 }

@@ -184,7 +184,7 @@ def _declare(lib):
     lib.rbp_net_train_step.restype = ct.c_int
     lib.rbp_net_train_step.argtypes = [P, i64, P, P, P, ct.POINTER(RbpNetHparams), P, P, P]
     lib.rbp_net_propose.restype = ct.c_int
-    lib.rbp_net_propose.argtypes = [P, i64, P, P, ct.c_float, ct.c_float, P, P, P]
+    lib.rbp_net_propose.argtypes = [P, i64, P, P, ct.c_float, ct.c_float, P, P, P, P, P]
     return lib
 
 

@@ -541,6 +541,8 @@ struct ProposeArgs {
   float lo, hi;
   float* gammas;            // [B, V] or null
   float* logits;            // [B, V] or null
+  const int32_t* shot_list;   // [B] shots to evaluate, or null: all
+  const int32_t* list_count;  // device count of shot_list entries, or null: B
   const bf16* theta;        // [N_PARAMS]
   const float* chk_lmean;   // [C] mean of the check's variables' tanh(llr/16)
   const uint16_t* graph16;  // chk_ptr [C+1], chk_var [E], var_ptr [V+1], var_chk [E]
@@ -653,7 +655,10 @@ __global__ void __launch_bounds__(PROPOSE_THREADS, 1) net_propose_kernel(NetGrap
     reinterpret_cast<uint4*>(sg)[i] = __ldg(reinterpret_cast<const uint4*>(pa.graph16) + i);
   __syncthreads();
 
-  for (long long b = blockIdx.x; b < pa.B; b += gridDim.x) {
+  const long long n_items = pa.shot_list && pa.list_count ? (long long)min(max(*pa.list_count, 0), (int)pa.B) : pa.B;
+  for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const long long b = pa.shot_list ? (long long)pa.shot_list[item] : item;
+    if (b < 0 || b >= pa.B) continue;  // block-uniform: no barrier is skipped by part of the block
     // variable features
     for (int c = tid; c < C; c += blockDim.x) s_syn[c] = pa.syn[b * C + c] & 1;
     __syncthreads();
@@ -1052,8 +1057,8 @@ int rbp_net_train_step(rbp_net* n, int64_t B, const uint8_t* syn, const float* p
   return RBP_OK;
 }
 
-int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float lo, float hi, float* gammas,
-                    float* logits, void* stream) {
+int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float lo, float hi,
+                    const int32_t* shot_list, const int32_t* list_count, float* gammas, float* logits, void* stream) {
   if (!n) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: null network");
   if (B < 0) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: negative batch");
   if (B == 0) return RBP_OK;
@@ -1072,6 +1077,8 @@ int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post
   pa.hi = hi;
   pa.gammas = gammas;
   pa.logits = logits;
+  pa.shot_list = shot_list;
+  pa.list_count = list_count;
   pa.theta = n->theta_bf.p;
   pa.chk_lmean = n->chk_lmean.p;
   pa.graph16 = n->graph16.p;

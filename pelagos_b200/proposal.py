@@ -149,15 +149,18 @@ class ProposalNet:
         B = syn.shape[0]
         g = torch.empty(B, self.decoder.V, dtype=torch.float32, device=self.device)
         r = torch.empty_like(g) if logits else None
-        nat.check(nat.lib().rbp_net_propose(self._h, B, _ptr(syn), _ptr(post), float(lo), float(hi), _ptr(g),
-                                            _ptr(r), self._stream()), "rbp_net_propose")
+        nat.check(nat.lib().rbp_net_propose(self._h, B, _ptr(syn), _ptr(post), float(lo), float(hi), None, None,
+                                            _ptr(g), _ptr(r), self._stream()), "rbp_net_propose")
         return (g, r) if logits else g
 
     def propose_into(self, B: int, syn: torch.Tensor, post: torch.Tensor, lo: float, hi: float,
-                     gammas: torch.Tensor) -> None:
-        """propose() into caller-owned device buffers (no reshaping, no allocation)."""
-        nat.check(nat.lib().rbp_net_propose(self._h, B, _ptr(syn), _ptr(post), float(lo), float(hi), _ptr(gammas),
-                                            None, self._stream()), "rbp_net_propose")
+                     gammas: torch.Tensor, shot_list: Optional[torch.Tensor] = None,
+                     list_count: Optional[torch.Tensor] = None) -> None:
+        """propose() into caller-owned device buffers (no reshaping, no allocation); with
+        ``shot_list`` / ``list_count`` (device int32) only those shots' rows are written."""
+        nat.check(nat.lib().rbp_net_propose(self._h, B, _ptr(syn), _ptr(post), float(lo), float(hi),
+                                            _ptr(shot_list), _ptr(list_count), _ptr(gammas), None, self._stream()),
+                  "rbp_net_propose")
 
     def train_step(self, syn, post, target, cfg: TrainConfig, lr: float, loss_out: Optional[torch.Tensor] = None,
                    grads_out: Optional[torch.Tensor] = None) -> None:
@@ -236,10 +239,16 @@ class LearnedRelayBPDecoder:
     pre-iterations (saving each shot's state and posterior), the network's
     tensor-core inference, and the relay legs resumed from the saved state with
     the proposed strengths on legs 0..learned_legs-1 and the seeded table after.
+    The relay legs take the shots the pre-iterations left unconverged first.
     Outputs have the same keys as ``RelayBPDecoder.decode``.
+
+    With ``gate=True`` the network is evaluated only for those unconverged
+    shots (chosen on the device, no host round trip); a shot the
+    pre-iterations solved keeps its posterior with the interval's top strength
+    ``hi`` on the learned legs.
     """
 
-    def __init__(self, decoder: RelayBPDecoder, net: ProposalNet, learned_legs: int = 4):
+    def __init__(self, decoder: RelayBPDecoder, net: ProposalNet, learned_legs: int = 4, gate: bool = False):
         if decoder.algo != "relay":
             raise ValueError("learned legs need algo='relay'")
         if decoder.num_gpus != 1:
@@ -247,6 +256,7 @@ class LearnedRelayBPDecoder:
         self.dec, self.net = decoder, net
         self.learned_legs = int(min(learned_legs, decoder.num_sets))
         self.lo, self.hi = (float(x) for x in decoder.gamma_dist_interval)
+        self.gate = bool(gate)
         self._bufs: Dict[int, dict] = {}
 
     def _buffers(self, B: int) -> dict:
@@ -261,6 +271,7 @@ class LearnedRelayBPDecoder:
                 "iters": torch.empty(B, dtype=torch.int32, device=dev),
                 "wfix": torch.empty(B, dtype=torch.int64, device=dev),
                 "errors": torch.empty(B, d.V, dtype=torch.uint8, device=dev),
+                "count": torch.empty(1, dtype=torch.int32, device=dev),
             }
             self._bufs = {B: b}  # keep one batch size
         return b
@@ -278,10 +289,17 @@ class LearnedRelayBPDecoder:
         pre_out = nat.RbpOutputs(found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]),
                                  last_posterior=_ptr(bf["post"]))
         d._native[gid].decode(B, pre_in, pre_out, stream)
-        self.net.propose_into(B, syn, bf["post"], self.lo, self.hi, bf["gammas"])
+        unsolved = bf["found"] == 0
+        order = torch.argsort((~unsolved).to(torch.uint8), stable=True).to(torch.int32)  # unconverged first
+        if self.gate:
+            bf["gammas"].fill_(self.hi)
+            bf["count"].copy_(unsolved.sum().to(torch.int32).view(1))
+            self.net.propose_into(B, syn, bf["post"], self.lo, self.hi, bf["gammas"], order, bf["count"])
+        else:
+            self.net.propose_into(B, syn, bf["post"], self.lo, self.hi, bf["gammas"])
         legs_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter,
                                gamma_legs_shot=_ptr(bf["gammas"]), n_shot_legs=self.learned_legs, shot_leg_rows=1,
-                               resume_state=_ptr(bf["state"]), legs_begin=0)
+                               resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order))
         legs_out = nat.RbpOutputs(errors=_ptr(bf["errors"]), weight_fixed=_ptr(bf["wfix"]),
                                   found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
         d._native[gid].decode(B, legs_in, legs_out, stream)
@@ -327,45 +345,80 @@ def _timed(fn):
     return out, e0.elapsed_time(e1)
 
 
+def constant_params(logit: float = 20.0) -> np.ndarray:
+    """Parameters of a network whose every output is sigmoid(logit): the constant-strength ablation."""
+    theta = np.zeros(param_count(), np.float32)
+    theta[-1] = logit
+    return theta
+
+
 def evaluate(workload, net: ProposalNet, decoder: RelayBPDecoder, shots: int, seed: int, chunk: int = 262144,
-             learned_legs: int = 4) -> dict:
-    """Plain and learned decodes of the same fresh seeded shots: logical error rate (Wilson 95%
-    interval), mean iterations and decode time of each (device time, syndromes resident)."""
+             learned_legs: int = 4, variants=("plain", "learned", "learned_gated", "constant_hi")) -> dict:
+    """Decode the same fresh seeded shots with each variant: logical error rate (Wilson 95% interval),
+    mean iterations and decode time (device time, syndromes resident, one call per chunk).
+
+    plain          the decoder alone (seeded legs)
+    learned        network strengths on legs 0..learned_legs-1 for every shot
+    learned_gated  network strengths for the shots the pre-iterations left unconverged, the top
+                   strength hi for the others
+    constant_hi    strength hi (a network with constant output) for every shot: the ablation
+    """
     from .experiments import wilson
 
-    learned = LearnedRelayBPDecoder(decoder, net, learned_legs=learned_legs)
-    rows = {"plain": {"fails": 0, "unconv": 0, "iters": 0, "ms": 0.0},
-            "learned": {"fails": 0, "unconv": 0, "iters": 0, "ms": 0.0}}
+    const_net = ProposalNet(decoder, constant_params())
+    runners = {
+        "plain": decoder.decode,
+        "learned": LearnedRelayBPDecoder(decoder, net, learned_legs).decode,
+        "learned_gated": LearnedRelayBPDecoder(decoder, net, learned_legs, gate=True).decode,
+        "constant_hi": LearnedRelayBPDecoder(decoder, const_net, learned_legs).decode,
+    }
+    rows = {v: {"fails": 0, "unconv": 0, "iters": 0, "ms": 0.0} for v in variants}
     done, k = 0, 0
+    gamma_stats = None
     while done < shots:
         n = min(chunk, shots - done)
         err, syn = workload.sample(n, seed=seed + k)
         syn_d = torch.from_numpy(syn).to(net.device)
         if k == 0:
-            decoder.decode(syn_d)
-            learned.decode(syn_d)
-        for name, fn in (("plain", lambda: decoder.decode(syn_d)), ("learned", lambda: learned.decode(syn_d))):
-            out, ms = _timed(fn)
-            o = {kk: v.cpu().numpy() for kk, v in out.items() if isinstance(v, torch.Tensor)}
+            for v in variants:
+                runners[v](syn_d)  # warm-up at this size
+            pre = decoder.decode_phases(syn_d, skip_relay_legs=True, return_last_posterior=True)
+            g = net.propose(syn_d, pre["last_posterior"], *decoder.gamma_dist_interval)
+            solved = pre["found_count"] > 0
+            gamma_stats = {"mean_gamma_solved": float(g[solved].mean()),
+                           "frac_below_0p6_solved": float((g[solved] < 0.6).float().mean()),
+                           "mean_gamma_unsolved": float(g[~solved].mean()) if bool((~solved).any()) else None,
+                           "frac_below_0p6_unsolved": float((g[~solved] < 0.6).float().mean())
+                           if bool((~solved).any()) else None,
+                           "unsolved_after_pre_iterations": int((~solved).sum())}
+        for v in variants:
+            out, ms = _timed(lambda: runners[v](syn_d))
+            o = {kk: x.cpu().numpy() for kk, x in out.items() if isinstance(x, torch.Tensor)}
             conv = o["found_count"] > 0
             f = workload.logical_failures(err, o["errors"], conv)
-            r = rows[name]
+            r = rows[v]
             r["fails"] += int(f.sum())
             r["unconv"] += int((~conv).sum())
             r["iters"] += int(o["iterations"].astype(np.int64).sum())
             r["ms"] += ms
         done += n
         k += 1
-    res = {"shots": shots, "seed": seed, "learned_legs": learned_legs}
-    for name, r in rows.items():
+    res = {"shots": shots, "seed": seed, "learned_legs": learned_legs, "chunk": chunk,
+           "network_outputs_first_chunk": gamma_stats}
+    for v, r in rows.items():
         lo, hi = wilson(r["fails"], shots)
-        res[name] = {"ler": r["fails"] / shots, "ler_ci95": [lo, hi], "failures": r["fails"],
-                     "unconverged": r["unconv"], "mean_iterations": r["iters"] / shots,
-                     "decode_ms": r["ms"], "shots_per_s": shots / (r["ms"] * 1e-3)}
-    res["speedup"] = res["learned"]["shots_per_s"] / res["plain"]["shots_per_s"]
-    res["iteration_ratio"] = res["plain"]["mean_iterations"] / res["learned"]["mean_iterations"]
-    pl, le = res["plain"]["ler_ci95"], res["learned"]["ler_ci95"]
-    res["ler_intervals_overlap"] = bool(le[0] <= pl[1] and pl[0] <= le[1])
+        res[v] = {"ler": r["fails"] / shots, "ler_ci95": [lo, hi], "failures": r["fails"],
+                  "unconverged": r["unconv"], "mean_iterations": r["iters"] / shots,
+                  "decode_ms": r["ms"], "shots_per_s": shots / (r["ms"] * 1e-3)}
+    if "plain" in rows:
+        pl = res["plain"]
+        for v in variants:
+            if v == "plain":
+                continue
+            res[v]["speedup_vs_plain"] = res[v]["shots_per_s"] / pl["shots_per_s"]
+            res[v]["iteration_ratio_vs_plain"] = pl["mean_iterations"] / res[v]["mean_iterations"]
+            ci = res[v]["ler_ci95"]
+            res[v]["ler_within_plain_ci"] = bool(ci[0] <= pl["ler_ci95"][1] and pl["ler_ci95"][0] <= ci[1])
     return res
 
 
