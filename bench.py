@@ -6,6 +6,12 @@ perfect round; H is 936 x 2,592 with 6,912 nonzeros; p = 0.003 on every column)
 with the full Relay-BP-S schedule (pre_iter 80, 100 relay legs of at most 60
 iterations, gamma0 0.65, leg gammas U(-0.24, 0.66), stop_nconv 5), float32.
 
+The decoder measured is the learned one: the pre-iterations, the proposal
+network (for the shots they leave unconverged) and the relay legs with the
+learned strengths on legs 0-3 (LearnedRelayBPDecoder, gate=True).  The plain
+decoder (RelayBPDecoder.decode, seeded legs) decodes the same shots in the same
+run and is reported under "plain", with both logical error rates.
+
   value  shots/s with the syndromes already in HBM (public decode() call on a
          device tensor), CUDA events on the launching stream, max over ranks;
   e2e    shots/s through the same decode() with pinned host syndromes: the
@@ -39,6 +45,7 @@ RELAY = dict(pre_iter=80, num_sets=100, set_max_iter=60, gamma0=0.65, gamma_dist
              stop_nconv=5, algo="relay", seed=1234)
 METRIC = "shots/s on one B200 at matched logical error rate, learned vs plain Relay-BP"
 CONFIG_NAME = "[[144,12,12]] BB phenomenological, 12 noisy + 1 perfect round, p=0.003, 65,536 shots"
+LEARNED_LEGS = 4
 
 
 def algorithmic_bytes_per_shot_iteration(C: int, V: int, E: int, msg_bytes: int = 4) -> int:
@@ -208,12 +215,15 @@ def main():
         pg = dist
 
     from pelagos_b200 import RelayBPDecoder, codes
+    from pelagos_b200.proposal import LearnedRelayBPDecoder, ProposalNet, default_weights_path, load_params
 
     w = codes.workload(WORKLOAD, p=P)
     shots = args.shots
     err, syn = w.sample(shots, seed=SEED + rank)
     launch = tuple(int(x) for x in args.launch.split(",")) if args.launch else None
     dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], launch=launch, **RELAY)
+    params, meta = load_params(default_weights_path(WORKLOAD, P))
+    learned = LearnedRelayBPDecoder(dec, ProposalNet(dec, params), learned_legs=LEARNED_LEGS, gate=True)
     syn_dev = torch.from_numpy(syn).to(dev)
     syn_pin = torch.from_numpy(syn).pin_memory()
     if launch is None and not args.no_autotune:
@@ -228,45 +238,49 @@ def main():
             pg.barrier()
         torch.cuda.synchronize()
 
-    clocks = ClockSampler(local).start()
-    # warm-up (untimed)
-    out = None
-    for _ in range(args.warmup):
-        out = dec.decode(syn_dev)
-        flush.zero_()
-    torch.cuda.synchronize()
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
 
-    # ---------------- device-resident timing: K steps in one bracket
-    iters_total = 0
-    barrier()
+    def timed_steps(fn, phases: bool):
+        """K steps bracketed by one pair of events (value); per-step events for the kernel times."""
+        for _ in range(args.warmup):
+            fn(None)
+            flush.zero_()
+        barrier()
+        t_start, t_end = ev(), ev()
+        step_ev = [[ev() for _ in range(4 if phases else 2)] for _ in range(args.steps)]
+        outs = []
+        t_start.record(stream)
+        for k in range(args.steps):
+            flush.zero_()
+            if not phases:
+                step_ev[k][0].record(stream)
+            o = fn(step_ev[k] if phases else None)
+            if not phases:
+                step_ev[k][1].record(stream)
+            outs.append(o)
+        t_end.record(stream)
+        barrier()
+        ms = t_start.elapsed_time(t_end) / args.steps
+        if pg is not None:
+            t = torch.tensor([ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        iters = sum(int(o["iterations"].sum().item()) for o in outs) / args.steps
+        return ms, step_ev, outs[-1], iters
+
+    clocks = ClockSampler(local).start()
     wall0 = time.time()
-    t_start = torch.cuda.Event(enable_timing=True)
-    t_end = torch.cuda.Event(enable_timing=True)
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    t_start.record(stream)
-    step_iters = []
-    for k in range(args.steps):
-        flush.zero_()
-        ev[k][0].record(stream)
-        o = dec.decode(syn_dev)
-        ev[k][1].record(stream)
-        step_iters.append(o["iterations"])
-        out = o
-    t_end.record(stream)
-    barrier()
+    # ---------------- the learned (gated) decode: the headline
+    ms_step, l_ev, out, l_iters = timed_steps(lambda e: learned.decode(syn_dev, events=e), phases=True)
+    decode_ms = [e[0].elapsed_time(e[1]) + e[2].elapsed_time(e[3]) for e in l_ev]
+    net_ms = [e[1].elapsed_time(e[2]) for e in l_ev]
+    # ---------------- the plain decode of the same shots
+    p_ms, p_ev, p_out, p_iters = timed_steps(lambda e: dec.decode(syn_dev), phases=False)
     wall1 = time.time()
     clocks.stop()
-    total_ms = t_start.elapsed_time(t_end)
-    kern_ms = [a.elapsed_time(b) for a, b in ev]
-    for it in step_iters:
-        iters_total += int(it.sum().item())
-    print("per-step ms: " + " ".join(f"{x:.2f}" for x in kern_ms), file=sys.stderr)
-    ms_step = total_ms / args.steps
-    if pg is not None:
-        t = torch.tensor([ms_step], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_step = float(t.item())
     value = world * shots / (ms_step / 1000.0)
+    print("learned per-step ms: " + " ".join(f"{a + b:.2f}" for a, b in zip(decode_ms, net_ms)), file=sys.stderr)
 
     # ---------------- end-to-end through the public API with host buffers
     V = w.H.shape[1]
@@ -280,11 +294,10 @@ def main():
     h2d = syn_pin.numel() * syn_pin.element_size()
     e2e_steps = max(1, min(args.steps, 3))
     barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    e0, e1 = ev(), ev()
     e0.record(stream)
     for _ in range(e2e_steps):
-        o = dec.decode(syn_pin)
+        o = learned.decode(syn_pin)
         for k, t in res_pin.items():
             t.copy_(o[k], non_blocking=True)
     e1.record(stream)
@@ -295,46 +308,53 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = world * shots / (e2e_ms / 1000.0)
-    from pelagos_b200.decoder import HARD_FIRST_MIN_BATCH
-
-    # the relay decode of a large batch is two launches: pre-iterations, then relay legs hardest-first
-    launches_per_decode = 2 if (dec.hard_shots_first and shots >= HARD_FIRST_MIN_BATCH) else 1
 
     if rank == 0:
-        last = {k: v.cpu().numpy() for k, v in out.items() if isinstance(v, torch.Tensor)}
-        conv = last["found_count"] > 0
-        fails = w.logical_failures(err, last["errors"], conv)
-        ler = float(fails.mean())
-        lo_ci, hi_ci = _wilson(int(fails.sum()), shots)
-        mean_it = iters_total / (args.steps * shots)
+        def ler(o):
+            o = {k: v.cpu().numpy() for k, v in o.items() if isinstance(v, torch.Tensor)}
+            conv = o["found_count"] > 0
+            f = w.logical_failures(err, o["errors"], conv)
+            lo_ci, hi_ci = _wilson(int(f.sum()), shots)
+            return {"value": float(f.mean()), "failures": int(f.sum()), "ci95": [lo_ci, hi_ci], "shots": shots,
+                    "unconverged": int((~conv).sum()), "mean_iterations": float(o["iterations"].mean())}
+
+        l_ler, p_ler = ler(out), ler(p_out)
         bps = algorithmic_bytes_per_shot_iteration(w.H.shape[0], V, w.H.nnz,
                                                    {"float32": 4, "float64": 8}.get(args.dtype, 2))
-        kern = float(np.mean(kern_ms))
-        achieved = bps * (iters_total / args.steps) / (kern / 1000.0) / 1e9
+        kern = float(np.mean(decode_ms))
+        achieved = bps * l_iters / (kern / 1000.0) / 1e9  # the two decode launches of a step
         peaks = _peaks()
         clk = clocks.summary(wall0, wall1)
         sm_ghz = (clk["sm_mhz"] or 1965.0) / 1000.0
         smem_peak = torch.cuda.get_device_properties(local).multi_processor_count * 128 * sm_ghz
+        p_kern = float(np.mean([a.elapsed_time(b) for a, b in p_ev]))
         line = {
             "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"float32": "f32", "float16": "f16 msgs / f32 acc",
                                             "bfloat16": "bf16 msgs / f32 acc", "float64": "f64"}[args.dtype],
             "data": "synthetic (seeded i.i.d. Bernoulli(p) errors on every column, s = H e mod 2)",
-            "config": {"workload": CONFIG_NAME, "shots": shots, "p": P, "decoder": "plain Relay-BP-S (seeded legs)",
+            "config": {"workload": CONFIG_NAME, "shots": shots, "p": P,
+                       "decoder": f"Relay-BP-S with learned strengths on relay legs 0-{LEARNED_LEGS - 1} "
+                                  "(network evaluated for the shots the pre-iterations leave unconverged; "
+                                  "solved shots keep their posterior at the top strength), seeded legs after",
+                       "network": {"weights": default_weights_path(WORKLOAD, P).name,
+                                   "trained_tuples": meta.get("train", {}).get("tuples")},
                        "schedule": "pre_iter 80, num_sets 100, set_max_iter 60, gamma0 0.65, (-0.24,0.66), S=5",
-                       "queue": "pre-iterations, then relay legs with the unconverged shots first"
-                                if launches_per_decode == 2 else "one launch",
                        "l2": "256 MB buffer written between timed steps (flush)",
                        "launch": dec.launch_info()},
-            "logical_error_rate": {"value": ler, "ci95": [lo_ci, hi_ci], "shots": shots,
-                                   "unconverged": int((~conv).sum()), "mean_iterations": mean_it},
+            "logical_error_rate": l_ler,
+            "plain": {"value": world * shots / (p_ms / 1000.0), "unit": "shots/s", "ms_per_step": p_ms,
+                      "kernel_ms": p_kern, "logical_error_rate": p_ler,
+                      "note": "the same shots through RelayBPDecoder.decode (seeded legs), same run"},
+            "learned_over_plain": p_ms / ms_step,
+            "phase_ms": {"decode_kernel": kern, "network_and_selection": float(np.mean(net_ms))},
             "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps * launches_per_decode,
+            "gpu_launches": args.steps * 3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm"], "traffic": None,
-                         "kernel": "relaybp_decode_kernel", "kernel_ms": kern,
-                         "bytes_per_shot_iteration": bps, "shot_iterations_per_launch": iters_total / args.steps,
+                         "kernel": "relaybp_decode_kernel (pre-iterations + relay legs of one step)",
+                         "kernel_ms": kern, "bytes_per_shot_iteration": bps, "shot_iterations_per_step": l_iters,
                          "peak_source": peaks["source"],
                          "smem": {"peak": smem_peak, "frac": achieved / smem_peak,
                                   "note": "SMs x 128 B/clk x median SM clock; messages live in shared memory"}},

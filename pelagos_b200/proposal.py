@@ -276,19 +276,25 @@ class LearnedRelayBPDecoder:
             self._bufs = {B: b}  # keep one batch size
         return b
 
-    def decode_into(self, syn: torch.Tensor) -> dict:
-        """Launch the three phases into the persistent buffers of this batch size (no host sync)."""
+    def decode_into(self, syn: torch.Tensor, events=None) -> dict:
+        """Launch the three phases into the persistent buffers of this batch size (no host sync).
+        ``events``: four CUDA events recorded before the pre-iterations, after them, after the
+        network (with its shot selection) and after the relay legs."""
         d = self.dec
         B = int(syn.shape[0])
         bf = self._buffers(B)
         gid = d.device_ids[0]
         stream = torch.cuda.current_stream(self.net.device).cuda_stream
         gamma0 = float(np.float32(d.gamma0))
+        if events is not None:
+            events[0].record()
         pre_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter, skip_relay_legs=1,
                               suspend_state=_ptr(bf["state"]))
         pre_out = nat.RbpOutputs(found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]),
                                  last_posterior=_ptr(bf["post"]))
         d._native[gid].decode(B, pre_in, pre_out, stream)
+        if events is not None:
+            events[1].record()
         unsolved = bf["found"] == 0
         order = torch.argsort((~unsolved).to(torch.uint8), stable=True).to(torch.int32)  # unconverged first
         if self.gate:
@@ -302,17 +308,21 @@ class LearnedRelayBPDecoder:
                                resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order))
         legs_out = nat.RbpOutputs(errors=_ptr(bf["errors"]), weight_fixed=_ptr(bf["wfix"]),
                                   found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
+        if events is not None:
+            events[2].record()
         d._native[gid].decode(B, legs_in, legs_out, stream)
+        if events is not None:
+            events[3].record()
         return bf
 
-    def decode(self, syndromes: torch.Tensor) -> Dict[str, torch.Tensor]:
+    def decode(self, syndromes: torch.Tensor, events=None) -> Dict[str, torch.Tensor]:
         d = self.dec
         syn = syndromes.to(device=self.net.device, dtype=torch.uint8).contiguous()
         if syn.ndim != 2 or syn.shape[1] != d.C:
             raise ValueError(f"syndromes must be [B, {d.C}]")
         if syn.shape[0] == 0:
             return d.decode(syn)
-        bf = self.decode_into(syn)
+        bf = self.decode_into(syn, events)
         wfix, found = bf["wfix"].clone(), bf["found"].clone()
         has = wfix != torch.iinfo(torch.int64).max
         weights = torch.where(has, wfix.to(torch.float64) * (2.0 ** -32),
