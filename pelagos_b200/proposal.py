@@ -455,9 +455,22 @@ def main(argv=None):
     e.add_argument("--shots", type=int, default=1 << 20)
     e.add_argument("--seed", type=int, default=900001)
     e.add_argument("--out", default=None)
+    c = sub.add_parser("propose-case", help="a small inference case: pre-iterations, then the network 3 times")
+    c.add_argument("--workload", default="bb144_phen")
+    c.add_argument("--p", type=float, default=0.003)
+    c.add_argument("--shots", type=int, default=4096)
     a = ap.parse_args(argv)
     w = codes.workload(a.workload, p=a.p)
     dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    if a.cmd == "propose-case":
+        net = ProposalNet(dec, load_params(default_weights_path(a.workload, a.p))[0])
+        syn = torch.from_numpy(w.sample(a.shots, seed=1)[1]).to(net.device)
+        pre = dec.decode_phases(syn, skip_relay_legs=True, return_last_posterior=True)
+        for _ in range(3):
+            g = net.propose(syn, pre["last_posterior"], *dec.gamma_dist_interval)
+        torch.cuda.synchronize()
+        print(json.dumps({"shots": a.shots, "mean_gamma": float(g.mean())}))
+        return
     if a.cmd == "train":
         cfg = TrainConfig(tuples=a.tuples, batch=a.batch, lr=a.lr, w_neg=a.w_neg, seed=a.seed)
         net, hist = train(dec, w.H, w.priors, cfg)
