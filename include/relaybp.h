@@ -146,6 +146,16 @@ typedef struct {
    * on it; putting the shots that will run longest first keeps them from
    * finishing after everything else.  Entries outside [0, B) are skipped. */
   const int32_t* shot_order;
+  /* Device int32: only queue positions below it are taken (NULL: all B). */
+  const int32_t* queue_len;
+  /* Split decode.  After the pre-iterations, a shot that found a solution runs
+   * relay legs l < solved_legs with the constant strength solved_gamma; with
+   * suspend_unsolved = 1 (which needs suspend_state) a shot that found none
+   * saves its state there and stops, to be resumed by a later call, and only
+   * such shots write their state. */
+  float solved_gamma;
+  int32_t solved_legs;
+  int32_t suspend_unsolved;
 } rbp_batch;
 
 /* Outputs (device memory).  Any may be NULL except found_count/iterations. */
@@ -161,6 +171,9 @@ typedef struct {
 
 /* Bytes of one shot's saved state (rbp_batch.resume_state / suspend_state). */
 RBP_API int rbp_state_bytes(const rbp_decoder* d, int64_t* bytes_per_shot);
+
+/* Byte offset of the posterior ([V] f32, f64 for RBP_MSG_F64) inside a saved state. */
+RBP_API int rbp_state_posterior_offset(const rbp_decoder* d, int64_t* offset);
 
 /*
  * Decode B shots on `stream`.  Asynchronous: returns after the launch.
@@ -296,15 +309,17 @@ RBP_API int rbp_net_train_step(rbp_net* n, int64_t B, const uint8_t* syn, const 
                                const rbp_net_hparams* hp, float* loss, float* grads, void* stream);
 
 /* Inference on the tensor cores: gammas [B, V] = lo + (hi - lo) sigmoid(r) and/or
- * logits [B, V].  With shot_list (device [B]) only the shots shot_list[i],
+ * logits [B, V].  Shot b's posterior is post[b * post_stride ...] (post_stride
+ * 0: V), so it can be read straight out of saved decode states
+ * (rbp_state_posterior_offset).  With shot_list (device [B]) only the shots shot_list[i],
  * i < *list_count (a device int32; all B entries when list_count is NULL),
  * are evaluated and their rows written; other rows are left as they are, so a
  * caller can evaluate a subset chosen on the device without a host round trip.
  * Needs a graph below 65536 edges whose per-shot state fits in one block's
  * shared memory (RBP_ERR_UNSUPPORTED otherwise). */
-RBP_API int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float lo, float hi,
-                            const int32_t* shot_list, const int32_t* list_count, float* gammas, float* logits,
-                            void* stream);
+RBP_API int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, int64_t post_stride,
+                            float lo, float hi, const int32_t* shot_list, const int32_t* list_count, float* gammas,
+                            float* logits, void* stream);
 
 #ifdef __cplusplus
 }

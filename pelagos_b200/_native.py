@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = (
     "rbp_decoder_configure",
     "rbp_decoder_query",
     "rbp_state_bytes",
+    "rbp_state_posterior_offset",
     "rbp_decode",
     "rbp_decode_static",
     "rbp_mixed_create",
@@ -98,6 +99,10 @@ class RbpBatch(ct.Structure):
         ("legs_end", ct.c_int32),
         ("shot_leg_rows", ct.c_int32),
         ("shot_order", ct.c_void_p),
+        ("queue_len", ct.c_void_p),
+        ("solved_gamma", ct.c_float),
+        ("solved_legs", ct.c_int32),
+        ("suspend_unsolved", ct.c_int32),
     ]
 
 
@@ -152,6 +157,8 @@ def _declare(lib):
     lib.rbp_decoder_query.argtypes = [P, ct.POINTER(i64), ct.POINTER(i64), i32p, i32p, i32p]
     lib.rbp_state_bytes.restype = ct.c_int
     lib.rbp_state_bytes.argtypes = [P, ct.POINTER(i64)]
+    lib.rbp_state_posterior_offset.restype = ct.c_int
+    lib.rbp_state_posterior_offset.argtypes = [P, ct.POINTER(i64)]
     lib.rbp_decode.restype = ct.c_int
     lib.rbp_decode.argtypes = [P, i64, ct.POINTER(RbpBatch), ct.POINTER(RbpOutputs), P]
     lib.rbp_decode_static.restype = ct.c_int
@@ -184,7 +191,7 @@ def _declare(lib):
     lib.rbp_net_train_step.restype = ct.c_int
     lib.rbp_net_train_step.argtypes = [P, i64, P, P, P, ct.POINTER(RbpNetHparams), P, P, P]
     lib.rbp_net_propose.restype = ct.c_int
-    lib.rbp_net_propose.argtypes = [P, i64, P, P, ct.c_float, ct.c_float, P, P, P, P, P]
+    lib.rbp_net_propose.argtypes = [P, i64, P, P, i64, ct.c_float, ct.c_float, P, P, P, P, P]
     return lib
 
 

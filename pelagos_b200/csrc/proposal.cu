@@ -537,7 +537,8 @@ __device__ uint32_t fragment_word(const bf16* th, int w) {
 struct ProposeArgs {
   long long B;
   const uint8_t* syn;       // [B, C]
-  const float* post;        // [B, V]
+  const float* post;        // row b at post + b * post_stride
+  long long post_stride;    // elements between rows (>= V)
   float lo, hi;
   float* gammas;            // [B, V] or null
   float* logits;            // [B, V] or null
@@ -663,7 +664,7 @@ __global__ void __launch_bounds__(PROPOSE_THREADS, 1) net_propose_kernel(NetGrap
     for (int c = tid; c < C; c += blockDim.x) s_syn[c] = pa.syn[b * C + c] & 1;
     __syncthreads();
     for (int v = tid; v < V; v += blockDim.x) {
-      const float pc = fminf(fmaxf(pa.post[b * V + v], -1e4f), 1e4f);
+      const float pc = fminf(fmaxf(pa.post[b * pa.post_stride + v], -1e4f), 1e4f);
       int cnt = 0;
       for (int k = var_ptr[v]; k < var_ptr[v + 1]; ++k) cnt += s_syn[var_chk[k]];
       s_th[v] = tanhf(pc * 0.0625f);
@@ -1057,13 +1058,15 @@ int rbp_net_train_step(rbp_net* n, int64_t B, const uint8_t* syn, const float* p
   return RBP_OK;
 }
 
-int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, float lo, float hi,
-                    const int32_t* shot_list, const int32_t* list_count, float* gammas, float* logits, void* stream) {
+int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post, int64_t post_stride, float lo,
+                    float hi, const int32_t* shot_list, const int32_t* list_count, float* gammas, float* logits,
+                    void* stream) {
   if (!n) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: null network");
   if (B < 0) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: negative batch");
   if (B == 0) return RBP_OK;
   if (!syn || !post || (!gammas && !logits)) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: null buffer");
   if (!(lo <= hi)) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: lo must not exceed hi");
+  if (post_stride != 0 && post_stride < n->V) return fail(RBP_ERR_ARGUMENT, "rbp_net_propose: post_stride below V");
   if (n->propose_blocks == 0)
     return fail(RBP_ERR_UNSUPPORTED, "rbp_net_propose: the graph and a shot's state (" +
                                          std::to_string(n->propose_smem) +
@@ -1073,6 +1076,7 @@ int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const float* post
   pa.B = B;
   pa.syn = syn;
   pa.post = post;
+  pa.post_stride = post_stride ? post_stride : n->V;
   pa.lo = lo;
   pa.hi = hi;
   pa.gammas = gammas;

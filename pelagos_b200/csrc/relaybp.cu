@@ -201,6 +201,9 @@ int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outpu
   if (in->n_shot_legs < 0 || (in->n_shot_legs > 0 && !in->gamma_legs_shot))
     return fail(RBP_ERR_ARGUMENT, w + ": gamma_legs_shot missing");
   if (in->shot_leg_rows < 0) return fail(RBP_ERR_ARGUMENT, w + ": shot_leg_rows must be >= 0");
+  if (in->solved_legs < 0) return fail(RBP_ERR_ARGUMENT, w + ": solved_legs must be >= 0");
+  if (in->suspend_unsolved && !in->suspend_state)
+    return fail(RBP_ERR_ARGUMENT, w + ": suspend_unsolved needs suspend_state");
   if (in->resume_state && (in->legs_begin < 0 || in->legs_begin > p.num_sets))
     return fail(RBP_ERR_ARGUMENT, w + ": legs_begin out of range");
   if ((reinterpret_cast<uintptr_t>(in->resume_state) | reinterpret_cast<uintptr_t>(in->suspend_state)) % 16)
@@ -236,6 +239,10 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.n_shot_legs = in->n_shot_legs;
   a.shot_leg_rows = in->shot_leg_rows > 0 ? in->shot_leg_rows : std::max(1, in->n_shot_legs);
   a.order = in->shot_order;
+  a.queue_len = in->queue_len;
+  a.solved_gamma = in->solved_gamma;
+  a.solved_legs = in->solved_legs;
+  a.suspend_unsolved = in->suspend_unsolved;
   a.init_post = in->init_posterior;
   a.errors = out->errors;
   a.errors_packed = out->errors_packed;
@@ -477,6 +484,12 @@ int rbp_state_bytes(const rbp_decoder* d, int64_t* bytes_per_shot) {
   return RBP_OK;
 }
 
+int rbp_state_posterior_offset(const rbp_decoder* d, int64_t* offset) {
+  if (!d || !offset) return fail(RBP_ERR_ARGUMENT, "rbp_state_posterior_offset: null argument");
+  *offset = rbpk::state_post_offset(d->g->V);
+  return RBP_OK;
+}
+
 int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem, int32_t* group_threads,
                       int32_t* groups_per_block, int32_t* blocks) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_query: null decoder");
@@ -567,6 +580,10 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.n_shot_legs = in->n_shot_legs;
     a.shot_leg_rows = in->shot_leg_rows > 0 ? in->shot_leg_rows : std::max(1, in->n_shot_legs);
     a.order = in->shot_order;
+    a.queue_len = in->queue_len;
+    a.solved_gamma = in->solved_gamma;
+    a.solved_legs = in->solved_legs;
+    a.suspend_unsolved = in->suspend_unsolved;
     a.init_post = in->init_posterior;
     a.errors = out->errors;
     a.errors_packed = out->errors_packed;

@@ -193,6 +193,12 @@ struct DevArgs {
   // scheduling
   int* queue;
   const int* order;              // [B] queue position -> shot index, or null (identity)
+  const int* queue_len;          // device count of queue positions to take, or null: B
+  // split decode: after the pre-iterations a solved shot runs relay legs < solved_legs at the
+  // constant strength solved_gamma; with suspend_unsolved an unsolved shot saves its state and stops
+  float solved_gamma;
+  int solved_legs;
+  int suspend_unsolved;
   int group_threads, groups;
   // shared-memory layout (byte offsets)
   int off_chk_deg, off_llr, off_group0, group_bytes;
@@ -410,8 +416,9 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
   while (true) {
     if (t == 0) {
       const long long q = (long long)atomicAdd(a.queue, 1);
-      long long sb = q;
-      if (q < a.B && a.order) {
+      const long long qn = a.queue_len ? (long long)max(0, min(*a.queue_len, (int)a.B)) : a.B;
+      long long sb = q < qn ? q : a.B;
+      if (q < qn && a.order) {
         sb = (long long)a.order[q];
         if (sb < 0 || sb >= a.B) sb = -1;  // not a shot index: this queue entry is skipped
       }
@@ -474,6 +481,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
       }
     }
     const int legs_stop = (a.legs_end > 0 && a.legs_end < a.num_sets) ? a.legs_end : a.num_sets;
+    bool solved_pre = false, stopped_unsolved = false;
 
     // Phase -1: the pre-iterations (decoder.py:3480-3616); phase l >= 0: relay
     // leg l (decoder.py:3672-3837).  A resumed shot starts at leg legs_begin.
@@ -492,6 +500,10 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         grow = (a.gamma_legs_shot && phase < a.n_shot_legs)
                    ? a.gamma_legs_shot + (b * (long long)a.shot_leg_rows + min(phase, a.shot_leg_rows - 1)) * V
                    : a.gamma_legs + (long long)phase * V;
+        if (solved_pre && phase < a.solved_legs) {
+          grow = nullptr;
+          gs = a.solved_gamma;
+        }
       }
 
       if (max_iter <= 0) {
@@ -690,11 +702,18 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         group_sync(bar, G);
       }
       if (phase < 0 && (found >= S || a.skip_legs)) break;
+      if (phase < 0) {
+        solved_pre = found > 0;
+        if (!solved_pre && a.suspend_unsolved) {
+          stopped_unsolved = true;
+          break;
+        }
+      }
     }
 
     // ---------------- outputs, decoder.py:3839-3873
     group_sync(bar, G);
-    if (a.suspend) {
+    if (a.suspend && (!a.suspend_unsolved || stopped_unsolved)) {
       unsigned char* st = a.suspend + b * (long long)a.state_stride;
       if (t == 0) {
         int* hdr = reinterpret_cast<int*>(st);

@@ -135,7 +135,8 @@ def test_learned_decode_matches_oracle_emulation(setup):
     np.testing.assert_array_equal((H @ out["errors"][ok].T.astype(np.int64) % 2).T, s["syn"][ok])
 
 
-def test_gated_decode_matches_oracle_emulation(setup):
+@pytest.mark.parametrize("fused", [False, True])
+def test_gated_decode_matches_oracle_emulation(setup, fused):
     """gate=True: shots the pre-iterations solved get the top strength on legs 0-3, the others the
     network's proposal; each equals the oracle run with those rows."""
     s = setup
@@ -144,7 +145,8 @@ def test_gated_decode_matches_oracle_emulation(setup):
     syn = w.sample(768, seed=9)[1]
     syn_d = torch.from_numpy(syn).to(DEV)
     net = ProposalNet(dec, s["theta"])
-    out = {k: v.cpu().numpy() for k, v in LearnedRelayBPDecoder(dec, net, gate=True).decode(syn_d).items()}
+    learned = LearnedRelayBPDecoder(dec, net, gate=True, fused=fused)
+    out = {k: v.cpu().numpy() for k, v in learned.decode(syn_d).items()}
     pre = dec.decode_phases(syn_d, skip_relay_legs=True, return_last_posterior=True)
     solved = pre["found_count"].cpu().numpy() > 0
     assert solved.any() and (~solved).any()
@@ -156,6 +158,22 @@ def test_gated_decode_matches_oracle_emulation(setup):
                    gamma0=dec.gamma0, gamma_legs=dec._leg_table(0), gamma_legs_shot=rows)
     for k in ("errors", "found_count", "iterations", "weight_fixed", "valid_mask"):
         np.testing.assert_array_equal(out[k], ref[k], err_msg=k)
+
+
+def test_graph_replay_equals_eager(setup):
+    """The captured learned decode gives the eager results, on refilled inputs too."""
+    s = setup
+    w = codes.workload("bb144_phen", p=0.005)
+    dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    net = ProposalNet(dec, s["theta"])
+    eager = LearnedRelayBPDecoder(dec, net, gate=True, graph=False)
+    graphed = LearnedRelayBPDecoder(dec, net, gate=True, graph=True)
+    for seed in (21, 22):
+        syn = torch.from_numpy(w.sample(2048, seed=seed)[1]).to(DEV)
+        a = {k: v.cpu().numpy() for k, v in eager.decode(syn).items()}
+        b = {k: v.cpu().numpy() for k, v in graphed.decode(syn).items()}
+        for k in a:
+            np.testing.assert_array_equal(a[k], b[k], err_msg=k)
 
 
 def test_training_lowers_the_loss(setup):
