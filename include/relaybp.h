@@ -321,6 +321,16 @@ RBP_API int rbp_net_propose(rbp_net* n, int64_t B, const uint8_t* syn, const flo
                             float lo, float hi, const int32_t* shot_list, const int32_t* list_count, float* gammas,
                             float* logits, void* stream);
 
+/*
+ * GF(2) product of a sparse 0/1 matrix (device CSR: row_ptr [R+1], cols) with
+ * each of B rows of x (device uint8 [B, N], only bit 0 read): out[b, r] =
+ * XOR_{j in row r} x[b, j] (device uint8 [B, R]).  Replaces the host-side
+ * products of the reference's observable runner, s = H e and O e
+ * (src/pelagos/adapter.py:545-560, 601-613, 679).  N <= 49,152.
+ */
+RBP_API int rbp_gf2_matvec(const uint8_t* x, int64_t B, int32_t N, const int32_t* row_ptr, const int32_t* cols,
+                           int32_t R, uint8_t* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,7 +6,9 @@ argument handling, graph preparation, seeded gamma tables and result
 assembly, mirroring the reference's Python interface.
 """
 
+from .adapter import DecodeResult, ObservableDecoderRunner, RelayDecoder, RelayDecoderF32, RelayDecoderF64
 from .decoder import RelayBPDecoder, UNCONVERGED_CORRECTIONS
 
-__all__ = ["RelayBPDecoder", "UNCONVERGED_CORRECTIONS"]
+__all__ = ["RelayBPDecoder", "UNCONVERGED_CORRECTIONS", "RelayDecoder", "RelayDecoderF32", "RelayDecoderF64",
+           "ObservableDecoderRunner", "DecodeResult"]
 __version__ = "0.1.0"

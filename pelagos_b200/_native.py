@@ -57,6 +57,7 @@ EXPORTED_SYMBOLS = (
     "rbp_net_forward",
     "rbp_net_train_step",
     "rbp_net_propose",
+    "rbp_gf2_matvec",
 )
 
 #: Bytes of the static scratch array rbp_decode_static uses (RBP_STATIC_SCRATCH_BYTES).
@@ -192,6 +193,8 @@ def _declare(lib):
     lib.rbp_net_train_step.argtypes = [P, i64, P, P, P, ct.POINTER(RbpNetHparams), P, P, P]
     lib.rbp_net_propose.restype = ct.c_int
     lib.rbp_net_propose.argtypes = [P, i64, P, P, i64, ct.c_float, ct.c_float, P, P, P, P, P]
+    lib.rbp_gf2_matvec.restype = ct.c_int
+    lib.rbp_gf2_matvec.argtypes = [P, i64, i32, P, P, i32, P, P]
     return lib
 
 
