@@ -47,6 +47,10 @@ RELAY = dict(pre_iter=80, num_sets=100, set_max_iter=60, gamma0=0.65, gamma_dist
 METRIC = "shots/s on one B200 at matched logical error rate, learned vs plain Relay-BP"
 CONFIG_NAME = "[[144,12,12]] BB phenomenological, 12 noisy + 1 perfect round, p=0.003, 65,536 shots"
 LEARNED_LEGS = 4
+# DRAM bytes (read + write) of the two decode-kernel launches of one learned decode, per shot: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum on 16,384 shots of this workload
+# (python -m pelagos_b200.experiments decode-case --shots 16384 --learned), 707,660,032 B / 16,384.
+DECODE_DRAM_BYTES_PER_SHOT = 43192
 
 
 def algorithmic_bytes_per_shot_iteration(C: int, V: int, E: int, msg_bytes: int = 4) -> int:
@@ -362,7 +366,10 @@ def main():
             "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * 3,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm"], "traffic": None,
+                         "frac": achieved / peaks["hbm"], "traffic": DECODE_DRAM_BYTES_PER_SHOT * shots,
+                         "traffic_note": "ncu DRAM bytes of a 16,384-shot learned decode's two decode launches, "
+                                         "scaled per shot; far below the algorithmic bytes because each shot's "
+                                         "messages stay in shared memory",
                          "kernel": "relaybp_decode_kernel (pre-iterations + relay legs of one step)",
                          "kernel_ms": kern, "bytes_per_shot_iteration": bps, "shot_iterations_per_step": l_iters,
                          "peak_source": peaks["source"],

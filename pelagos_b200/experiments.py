@@ -84,6 +84,26 @@ def precision_sweep(shots: int = 131072, ps=(0.002, 0.003, 0.004), dtypes=("floa
     return rows
 
 
+def decode_case(shots: int, launch=(480, 1), learned: bool = False) -> None:
+    """A small profiling case: two decodes of the same seeded [[144,12,12]] phenomenological batch
+    (p = 0.003), with the plain decoder or the learned (gated) one run eagerly; either decode is
+    two decode-kernel launches (pre-iterations, relay legs), the learned one with the network
+    launch between them."""
+    w = codes.workload("bb144_phen", p=0.003)
+    syn = torch.from_numpy(w.sample(shots, seed=2026)[1]).cuda()
+    dec = RelayBPDecoder(w.H, w.priors, launch=launch, **RELAY)
+    run = dec.decode
+    if learned:
+        from .proposal import LearnedRelayBPDecoder, ProposalNet, default_weights_path, load_params
+
+        run = LearnedRelayBPDecoder(dec, ProposalNet(dec, load_params(default_weights_path())[0]), gate=True,
+                                    graph=False).decode
+    for _ in range(2):
+        out = run(syn)
+    torch.cuda.synchronize()
+    print(json.dumps({"shots": shots, "shot_iterations": int(out["iterations"].sum())}))
+
+
 def markdown(rows: list[dict]) -> str:
     out = ["| p | messages | LER [95% CI] | unconverged | mean iters | shots/s | same errors as f64 | "
            "same iterations | LLR err max | LLR err RMS (ref RMS) |", "|---|---|---|---|---|---|---|---|---|---|"]
@@ -99,12 +119,17 @@ def markdown(rows: list[dict]) -> str:
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["precision"])
+    ap.add_argument("what", choices=["precision", "decode-case"])
     ap.add_argument("--shots", type=int, default=131072)
+    ap.add_argument("--launch", default="480,1", help="decode-case: G,groups kernel shape")
+    ap.add_argument("--learned", action="store_true", help="decode-case: the learned (gated, eager) decode")
     ap.add_argument("--out", default=None)
     ap.add_argument("--dtypes", default="float64,float32,float16,bfloat16",
                     help="comma-separated; float64 (the reference run) must come first")
     args = ap.parse_args(argv)
+    if args.what == "decode-case":
+        decode_case(args.shots, tuple(int(x) for x in args.launch.split(",")), learned=args.learned)
+        return
     rows = precision_sweep(shots=args.shots, dtypes=tuple(args.dtypes.split(",")))
     md = markdown(rows)
     print(md)
