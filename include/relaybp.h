@@ -148,7 +148,8 @@ typedef struct {
   const int32_t* shot_order;
   /* Device int32: only queue positions below it are taken (NULL: all B). */
   const int32_t* queue_len;
-  /* Split decode.  After the pre-iterations, a shot that found a solution runs
+  /* Split decode.  After the pre-iterations (or when resumed at leg 0 with a
+   * solution found), a shot that found a solution runs
    * relay legs l < solved_legs with the constant strength solved_gamma; with
    * suspend_unsolved = 1 (which needs suspend_state) a shot that found none
    * saves its state there and stops, to be resumed by a later call, and only

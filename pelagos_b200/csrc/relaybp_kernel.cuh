@@ -482,6 +482,8 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
     }
     const int legs_stop = (a.legs_end > 0 && a.legs_end < a.num_sets) ? a.legs_end : a.num_sets;
     bool solved_pre = false, stopped_unsolved = false;
+    // a shot resumed at leg 0 was solved by the pre-iterations if it found a solution there
+    if (a.resume && a.legs_begin == 0) solved_pre = found > 0;
 
     // Phase -1: the pre-iterations (decoder.py:3480-3616); phase l >= 0: relay
     // leg l (decoder.py:3672-3837).  A resumed shot starts at leg legs_begin.

@@ -281,7 +281,6 @@ class LearnedRelayBPDecoder:
             d, dev = self.dec, self.net.device
             b = {
                 "state": d.new_state(B),
-                "post": torch.empty(B, d.V, dtype=torch.float32, device=dev),
                 "gammas": torch.empty(B, d.V, dtype=torch.float32, device=dev),
                 "found": torch.empty(B, dtype=torch.int32, device=dev),
                 "iters": torch.empty(B, dtype=torch.int32, device=dev),
@@ -328,22 +327,26 @@ class LearnedRelayBPDecoder:
             events[0].record()
         pre_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter, skip_relay_legs=1,
                               suspend_state=_ptr(bf["state"]))
-        pre_out = nat.RbpOutputs(found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]),
-                                 last_posterior=_ptr(bf["post"]))
+        pre_out = nat.RbpOutputs(found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
         d._native[gid].decode(B, pre_in, pre_out, stream)
         if events is not None:
             events[1].record()
         unsolved = bf["found"] == 0
         order = torch.argsort((~unsolved).to(torch.uint8), stable=True).to(torch.int32)  # unconverged first
+        post = bf["state"].data_ptr() + self._post_offset()  # posteriors, read from the saved states
+        stride = bf["state"].shape[1] // 4
         if self.gate:
-            bf["gammas"].fill_(self.hi)
+            # solved shots take the constant hi in the kernel; only unsolved rows are written
             bf["count"].copy_(unsolved.sum().to(torch.int32).view(1))
-            self.net.propose_into(B, syn, bf["post"], self.lo, self.hi, bf["gammas"], order, bf["count"])
+            self.net.propose_into(B, syn, post, self.lo, self.hi, bf["gammas"], order, bf["count"],
+                                  post_stride=stride)
         else:
-            self.net.propose_into(B, syn, bf["post"], self.lo, self.hi, bf["gammas"])
+            self.net.propose_into(B, syn, post, self.lo, self.hi, bf["gammas"], post_stride=stride)
         legs_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter,
                                gamma_legs_shot=_ptr(bf["gammas"]), n_shot_legs=self.learned_legs, shot_leg_rows=1,
-                               resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order))
+                               resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order),
+                               solved_gamma=float(np.float32(self.hi)),
+                               solved_legs=self.learned_legs if self.gate else 0)
         legs_out = nat.RbpOutputs(errors=_ptr(bf["errors"]), weight_fixed=_ptr(bf["wfix"]),
                                   found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
         if events is not None:
