@@ -59,6 +59,23 @@ def algorithmic_bytes_per_shot_iteration(C: int, V: int, E: int, msg_bytes: int 
     return 4 * E * msg_bytes + 13 * V + 2 * C
 
 
+def max_over_ranks(x: float, pg, device) -> float:
+    """The maximum of x over all ranks (x itself without a process group).  Step times are
+    reported as this maximum: a multi-GPU step ends when its slowest replica does."""
+    if pg is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_shots_per_s(world: int, shots_per_rank: int, ms_per_step: float) -> float:
+    """Weak scaling: every rank decodes its own batch, so the job decodes world x shots per step."""
+    return world * shots_per_rank / (ms_per_step / 1000.0)
+
+
 def _dist():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -266,11 +283,7 @@ def main():
             step_iters.append(o["iterations"])  # only the counts are kept across steps
         t_end.record(stream)
         barrier()
-        ms = t_start.elapsed_time(t_end) / args.steps
-        if pg is not None:
-            t = torch.tensor([ms], device=dev)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(t_start.elapsed_time(t_end) / args.steps, pg, dev)
         iters = sum(int(it.sum().item()) for it in step_iters) / args.steps
         return ms, step_ev, o, iters
 
@@ -292,7 +305,7 @@ def main():
     p_ms, p_ev, p_out, p_iters = timed_steps(lambda e: dec.decode(syn_dev), phases=False)
     wall1 = time.time()
     clocks.stop()
-    value = world * shots / (ms_step / 1000.0)
+    value = whole_job_shots_per_s(world, shots, ms_step)
     print("learned eager launches ms: " + " ".join(f"{a + b:.2f}" for a, b in zip(decode_ms, net_ms)), file=sys.stderr)
 
     # ---------------- end-to-end through the public API with host buffers
@@ -315,12 +328,8 @@ def main():
             t.copy_(o[k], non_blocking=True)
     e1.record(stream)
     barrier()
-    e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * shots / (e2e_ms / 1000.0)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, pg, dev)
+    e2e_value = whole_job_shots_per_s(world, shots, e2e_ms)
 
     if rank == 0:
         def ler(o):
@@ -357,7 +366,7 @@ def main():
                        "l2": "256 MB buffer written between timed steps (flush)",
                        "launch": dec.launch_info()},
             "logical_error_rate": l_ler,
-            "plain": {"value": world * shots / (p_ms / 1000.0), "unit": "shots/s", "ms_per_step": p_ms,
+            "plain": {"value": whole_job_shots_per_s(world, shots, p_ms), "unit": "shots/s", "ms_per_step": p_ms,
                       "kernel_ms": p_kern, "logical_error_rate": p_ler,
                       "note": "the same shots through RelayBPDecoder.decode (seeded legs), same run"},
             "learned_over_plain": p_ms / ms_step,
