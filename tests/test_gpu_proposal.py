@@ -222,3 +222,21 @@ def test_trained_network_gains_over_seeded_legs():
     assert f_gated <= f_plain and f_gated < f_const, (f_gated, f_plain, f_const)
     ok = gated["found_count"] > 0
     np.testing.assert_array_equal((w.H @ gated["errors"][ok].T.astype(np.int64) % 2).T, syn[ok])
+
+
+@pytest.mark.parametrize("dtype", ["bfloat16", "float16"])
+def test_learned_decode_with_16_bit_messages(dtype):
+    """The learned decode over a 16-bit-message decoder (float32 posteriors) matches the same
+    decoder run with the proposed strengths as per-shot leg rows."""
+    w = codes.workload("bb144_phen", p=0.005)
+    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, **RELAY)
+    from pelagos_b200.proposal import default_weights_path, load_params
+
+    net = ProposalNet(dec, load_params(default_weights_path())[0])
+    syn = torch.from_numpy(w.sample(2048, seed=31)[1]).to(DEV)
+    out = {k: v.cpu().numpy() for k, v in LearnedRelayBPDecoder(dec, net, gate=False).decode(syn).items()}
+    pre = dec.decode_phases(syn, skip_relay_legs=True, return_last_posterior=True)
+    gam = net.propose(syn, pre["last_posterior"], -0.24, 0.66)
+    ref = {k: v.cpu().numpy() for k, v in dec.decode(syn, leg_gammas=gam[:, None, :].expand(-1, 4, -1)).items()}
+    for k in ("errors", "found_count", "iterations", "weight_fixed"):
+        np.testing.assert_array_equal(out[k], ref[k], err_msg=k)
