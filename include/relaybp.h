@@ -157,6 +157,11 @@ typedef struct {
   float solved_gamma;
   int32_t solved_legs;
   int32_t suspend_unsolved;
+  /* When to test an iteration's parity before its min-sum pass, skipping that
+   * pass when every check holds: 0 never (one fused pass), 1 at the first
+   * testable iteration of each relay leg, 2 at every iteration.  Results do
+   * not depend on it; it pays off where legs converge at once. */
+  int32_t parity_first;
 } rbp_batch;
 
 /* Outputs (device memory).  Any may be NULL except found_count/iterations. */

@@ -104,6 +104,7 @@ class RbpBatch(ct.Structure):
         ("solved_gamma", ct.c_float),
         ("solved_legs", ct.c_int32),
         ("suspend_unsolved", ct.c_int32),
+        ("parity_first", ct.c_int32),
     ]
 
 

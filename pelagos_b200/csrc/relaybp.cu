@@ -202,6 +202,7 @@ int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outpu
     return fail(RBP_ERR_ARGUMENT, w + ": gamma_legs_shot missing");
   if (in->shot_leg_rows < 0) return fail(RBP_ERR_ARGUMENT, w + ": shot_leg_rows must be >= 0");
   if (in->solved_legs < 0) return fail(RBP_ERR_ARGUMENT, w + ": solved_legs must be >= 0");
+  if (in->parity_first < 0 || in->parity_first > 2) return fail(RBP_ERR_ARGUMENT, w + ": parity_first must be 0, 1 or 2");
   if (in->suspend_unsolved && !in->suspend_state)
     return fail(RBP_ERR_ARGUMENT, w + ": suspend_unsolved needs suspend_state");
   if (in->resume_state && (in->legs_begin < 0 || in->legs_begin > p.num_sets))
@@ -243,6 +244,7 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.solved_gamma = in->solved_gamma;
   a.solved_legs = in->solved_legs;
   a.suspend_unsolved = in->suspend_unsolved;
+  a.parity_first = in->parity_first;
   a.init_post = in->init_posterior;
   a.errors = out->errors;
   a.errors_packed = out->errors_packed;
@@ -584,6 +586,7 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.solved_gamma = in->solved_gamma;
     a.solved_legs = in->solved_legs;
     a.suspend_unsolved = in->suspend_unsolved;
+    a.parity_first = in->parity_first;
     a.init_post = in->init_posterior;
     a.errors = out->errors;
     a.errors_packed = out->errors_packed;

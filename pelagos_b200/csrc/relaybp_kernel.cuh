@@ -199,6 +199,7 @@ struct DevArgs {
   float solved_gamma;
   int solved_legs;
   int suspend_unsolved;
+  int parity_first;              // 0 never, 1 at iteration 1 of relay legs, 2 every iteration
   int group_threads, groups;
   // shared-memory layout (byte offsets)
   int off_chk_deg, off_llr, off_group0, group_bytes;
@@ -529,7 +530,41 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         for (int it = 0; it <= max_iter; ++it) {
           const bool check_parity = it > 0;
           const bool write_nu = it < max_iter;
+          // Parity first: test iteration it-1's hard decisions alone, and run the
+          // min-sum pass only if some check fails.  The nu a converged pass would
+          // write is never read (messages restart every leg), so results are the same.
+          const bool parity_first = check_parity && write_nu &&
+                                    (a.parity_first == 2 || (a.parity_first == 1 && phase >= 0 && it == 1));
           const A alpha = (a.use_alpha && write_nu) ? A(__ldg(a.alpha + it)) : A(1);
+          bool all_ok = false;
+          if (parity_first) {
+            bool okp = true;
+            int kp = 0;
+            for (int c = t; c < C; c += G, ++kp) {
+              const int s = (int)((synm >> kp) & 1u);
+              int par;
+              if constexpr (MAXDC > 0) {
+                constexpr int NQ = MAXDC / VecIO<M>::N;
+                constexpr int VEC = VecIO<M>::N;
+                const int deg = s_chk_deg[c];
+                const int swz = chunk_swizzle<M>(c);
+                uint32_t x = 0;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                  x ^= VecIO<M>::hard_word(hard + chunk_base<M>(q, c, C), deg - q * VEC, swz);
+                par = __popc(x) & 1;
+              } else {
+                const int deg = g.chk_ptr[c + 1] - g.chk_ptr[c];
+                int hp = 0;
+                for (int j = 0; j < deg; ++j) hp ^= hard[slot_index<M>(j, c, C)];
+                par = hp & 1;
+              }
+              okp = okp && (par == s);
+            }
+            all_ok = group_all(bar, G, okp);
+          }
+          if (!parity_first || !all_ok) {
+          const bool chk_par = check_parity && !parity_first;
 
           // ---------------- check pass (kernels.py:1052-1215) + parity of it-1 (kernels.py:510-569)
           bool ok_all = true;
@@ -549,7 +584,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
 #pragma unroll
               for (int q = 0; q < NQ; ++q)
                 VecIO<M>::load(msg + chunk_base<M>(q, c, C), mv + q * VecIO<M>::N);
-              if (check_parity) {
+              if (chk_par) {
                 uint32_t x = 0;
 #pragma unroll
                 for (int q = 0; q < NQ; ++q)
@@ -599,14 +634,14 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               for (int j = 0; j < deg; ++j) {
                 const int ix = slot_index<M>(j, c, C);
                 const A m = IO::ld(msg[ix]);
-                if (check_parity) hp ^= hard[ix];
+                if (chk_par) hp ^= hard[ix];
                 neg ^= (m < A(0)) ? 1 : 0;
                 const A x = fabs(m);
                 if (x < min1) { min2 = min1; min1 = x; cnt1 = 1; }
                 else if (x == min1) { cnt1 += 1; }
                 else if (x < min2) { min2 = x; }
               }
-              if (check_parity) ok_all = ok_all && ((hp & 1) == s);
+              if (chk_par) ok_all = ok_all && ((hp & 1) == s);
               if (write_nu) {
                 const bool par = ((neg ^ s) & 1) != 0;
                 for (int j = 0; j < deg; ++j) {
@@ -621,7 +656,9 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               }
             }
           }
-          const bool all_ok = group_all(bar, G, ok_all);
+          const bool a2 = group_all(bar, G, ok_all);
+          if (!parity_first) all_ok = a2;
+          }
 
           if (check_parity) {
             // check_and_select_kernel (kernels.py:609-741) for iteration it-1

@@ -144,6 +144,12 @@ class RelayBPDecoder:
       unconverged queued first.  Those few shots run up to
       pre_iter + num_sets * set_max_iter iterations; started first, they finish
       alongside the bulk instead of after it.  Results are identical.
+    * ``parity_first`` (default 2): when the kernel tests an iteration's parity
+      on its own before the min-sum pass, skipping that pass once every check
+      holds — 0 never (one fused pass), 1 at the first testable iteration of
+      each relay leg, 2 at every iteration.  Results are identical; 2 measured
+      fastest (27.4 vs 28.2 ms plain, 20.0 vs 21.3 ms learned, 65,536 shots of
+      the [[144,12,12]] phenomenological code).
     """
 
     def __init__(
@@ -180,6 +186,7 @@ class RelayBPDecoder:
         mix_rounding: str = "separate",
         launch: Optional[Tuple[int, int]] = None,
         hard_shots_first: bool = True,
+        parity_first: int = 2,
     ):
         if unconverged_correction not in UNCONVERGED_CORRECTIONS:
             raise ValueError(
@@ -278,6 +285,9 @@ class RelayBPDecoder:
 
         self._launch = tuple(launch) if launch is not None else None
         self.hard_shots_first = bool(hard_shots_first)
+        if parity_first not in (0, 1, 2):
+            raise ValueError("parity_first must be 0, 1 or 2")
+        self.parity_first = int(parity_first)
         self._native: Dict[int, _NativeDecoder] = {}
         self._legs_broadcast: Dict[int, torch.Tensor] = {}
         self._alpha_len = max(self.pre_iter, self.set_max_iter, 1)
@@ -633,7 +643,7 @@ class RelayBPDecoder:
                                  skip_relay_legs=1 if skip_relay_legs else 0,
                                  resume_state=_ptr(resume), suspend_state=_ptr(suspend),
                                  legs_begin=int(legs_begin), legs_end=int(legs_end), shot_leg_rows=shot_rows,
-                                 shot_order=_ptr(order))
+                                 shot_order=_ptr(order), parity_first=self.parity_first)
             outs = nat.RbpOutputs(errors=_ptr(errors), errors_packed=_ptr(packed), weights=None,
                                   weight_fixed=_ptr(wfix), found_count=_ptr(found), iterations=_ptr(iters),
                                   last_posterior=_ptr(last_post))

@@ -78,7 +78,8 @@ class MixedDecoder:
         outs = (nat.RbpOutputs * n)()
         for i, (d, buf) in enumerate(zip(self.decoders, self._bufs)):
             gamma0 = float(np.float32(d.gamma0)) if d.algo == "relay" else 0.0
-            ins[i] = nat.RbpBatch(syndromes=_ptr(buf["syndromes"]), gamma0=gamma0, pre_iter=d.pre_iter)
+            ins[i] = nat.RbpBatch(syndromes=_ptr(buf["syndromes"]), gamma0=gamma0, pre_iter=d.pre_iter,
+                                  parity_first=d.parity_first)
             outs[i] = nat.RbpOutputs(errors=_ptr(buf["errors"]), weight_fixed=_ptr(buf["weight_fixed"]),
                                      found_count=_ptr(buf["found_count"]), iterations=_ptr(buf["iterations"]))
         return Bs, ins, outs

@@ -326,7 +326,7 @@ class LearnedRelayBPDecoder:
         if events is not None:
             events[0].record()
         pre_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter, skip_relay_legs=1,
-                              suspend_state=_ptr(bf["state"]))
+                              suspend_state=_ptr(bf["state"]), parity_first=d.parity_first)
         pre_out = nat.RbpOutputs(found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
         d._native[gid].decode(B, pre_in, pre_out, stream)
         if events is not None:
@@ -346,7 +346,7 @@ class LearnedRelayBPDecoder:
                                gamma_legs_shot=_ptr(bf["gammas"]), n_shot_legs=self.learned_legs, shot_leg_rows=1,
                                resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order),
                                solved_gamma=float(np.float32(self.hi)),
-                               solved_legs=self.learned_legs if self.gate else 0)
+                               solved_legs=self.learned_legs if self.gate else 0, parity_first=d.parity_first)
         legs_out = nat.RbpOutputs(errors=_ptr(bf["errors"]), weight_fixed=_ptr(bf["wfix"]),
                                   found_count=_ptr(bf["found"]), iterations=_ptr(bf["iters"]))
         if events is not None:
