@@ -59,7 +59,7 @@ namespace {
 size_t msg_size(int t) { return t == RBP_MSG_F64 ? 8 : (t == RBP_MSG_F32 ? 4 : 2); }
 
 struct Layout {
-  int off_chk_deg, off_llr, off_group0;
+  int off_chk_deg, off_llr, off_first, off_group0;
   int g_msg, g_hard, g_best, g_first, g_red, group_bytes;
 };
 
@@ -88,6 +88,8 @@ Layout make_layout(int C, int V, int rows, int msg_type, int group_threads) {
   o = align16(o + C);
   L.off_llr = o;
   o = align16(o + 4 * V);
+  L.off_first = o;  // first-pass table of the check rows (see build_first_pass_table)
+  o = align16(o + (int)msg_size(msg_type) * rows * C);
   L.off_group0 = o;
   const int slots_total = rows * C + 1;  // + the dummy slot of absent variable edges
   const int W = (V + 31) / 32;
@@ -263,6 +265,8 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.groups = lc.groups;
   a.off_chk_deg = L.off_chk_deg;
   a.off_llr = L.off_llr;
+  a.off_first = L.off_first;
+  a.first_table = 1;
   a.off_group0 = L.off_group0;
   a.group_bytes = L.group_bytes;
   a.g_msg = L.g_msg;
@@ -605,6 +609,8 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.groups = m->NG[i];
     a.off_chk_deg = L.off_chk_deg;
     a.off_llr = L.off_llr;
+    a.off_first = L.off_first;
+    a.first_table = 1;
     a.off_group0 = L.off_group0;
     a.group_bytes = L.group_bytes;
     a.g_msg = L.g_msg;

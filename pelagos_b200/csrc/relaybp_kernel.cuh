@@ -202,7 +202,8 @@ struct DevArgs {
   int parity_first;              // 0 never, 1 at iteration 1 of relay legs, 2 every iteration
   int group_threads, groups;
   // shared-memory layout (byte offsets)
-  int off_chk_deg, off_llr, off_group0, group_bytes;
+  int off_chk_deg, off_llr, off_first, off_group0, group_bytes;
+  int first_table;               // 1: take each phase's first check pass from the block's table
   int g_msg, g_hard, g_best, g_first, g_red;
 };
 
@@ -356,6 +357,86 @@ __device__ __forceinline__ void ballot_post(const A (&post)[VPT], uint32_t* dst,
 // MAXDC check degree bound held in registers by the check pass (0: generic loop)
 // VPT   variables owned per thread
 // MAXDV variable degree bound (slot positions held in registers)
+// Negate every message of a 16-byte chunk (IEEE sign flip, exact in every
+// storage type: float16 / bfloat16 saturate and round symmetrically).
+template <typename M>
+__device__ __forceinline__ uint4 flip_signs(uint4 v) {
+  if constexpr (sizeof(M) == 2) {
+    v.x ^= 0x80008000u; v.y ^= 0x80008000u; v.z ^= 0x80008000u; v.w ^= 0x80008000u;
+  } else if constexpr (sizeof(M) == 4) {
+    v.x ^= 0x80000000u; v.y ^= 0x80000000u; v.z ^= 0x80000000u; v.w ^= 0x80000000u;
+  } else {
+    v.y ^= 0x80000000u; v.w ^= 0x80000000u;
+  }
+  return v;
+}
+
+// The first check pass of every phase reads mu_e = llr[var(e)]: it is the same
+// for every shot except for the syndrome bit, which only negates the check's
+// outputs (par flips, the magnitudes do not change).  This computes that pass
+// once per block for s = 0, with the same operations the check pass uses
+// (alpha of iteration 0, beta, the degree-1 rule, storage rounding), into the
+// table at off_first; the kernel then copies a row, negated when s = 1.
+template <typename M, int MAXDC>
+__device__ void build_first_pass_table(const DevGraph& g, const DevArgs& a, unsigned char* smem) {
+  if constexpr (MAXDC > 0) {
+    using IO = MsgT<M>;
+    using A = typename IO::A;
+    constexpr int VEC = VecIO<M>::N;
+    constexpr int NQ = MAXDC / VEC;
+    M* tab = reinterpret_cast<M*>(smem + a.off_first);
+    const float* s_llr = reinterpret_cast<const float*>(smem + a.off_llr);
+    const uint8_t* s_chk_deg = smem + a.off_chk_deg;
+    for (int v = threadIdx.x; v < g.V; v += blockDim.x)
+      for (int j = 0; j < g.vslots; ++j) {
+        const uint16_t p = g.var_pos[j * g.V + v];
+        if (p != kNoSlot) tab[p] = IO::st(A(s_llr[v]));
+      }
+    __syncthreads();
+    const A alpha = a.use_alpha ? A(__ldg(a.alpha)) : A(1);
+    const A beta = A(a.beta);
+    const A kInf = A(__int_as_float(0x7f800000));
+    for (int c = threadIdx.x; c < g.C; c += blockDim.x) {
+      const int deg = s_chk_deg[c];
+      const int swz = chunk_swizzle<M>(c);
+      A mv[MAXDC];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) VecIO<M>::load(tab + chunk_base<M>(q, c, g.C), mv + q * VEC);
+      int neg = 0;
+      A min1 = A(1e30), min2 = A(1e30);
+#pragma unroll
+      for (int j = 0; j < MAXDC; ++j) {
+        const bool in = ((j % VEC) ^ swz) < deg - (j / VEC) * VEC;
+        neg ^= (in && mv[j] < A(0)) ? 1 : 0;
+        const A x = in ? fmin(fabs(mv[j]), kInf) : kInf;
+        min2 = fmin(min2, fmax(min1, x));
+        min1 = fmin(min1, x);
+      }
+      const bool par = (neg & 1) != 0;  // syndrome bit 0
+      A lo = deg == 1 ? A(0) : min1;
+      A hi = deg == 1 ? A(0) : min2;
+      if (a.use_alpha) {
+        lo = mul_rn(alpha, lo);
+        hi = mul_rn(alpha, hi);
+      }
+      if (a.use_beta) {
+        lo = fmax(sub_rn(lo, beta), A(0));
+        hi = fmax(sub_rn(hi, beta), A(0));
+      }
+      A out[MAXDC];
+#pragma unroll
+      for (int j = 0; j < MAXDC; ++j) {
+        const A m = mv[j];
+        const A mag = (fabs(m) == min1) ? hi : lo;
+        out[j] = (par != !(m >= A(0))) ? -mag : mag;
+      }
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) VecIO<M>::store(tab + chunk_base<M>(q, c, g.C), out + q * VEC);
+    }
+    __syncthreads();
+  }
+}
+
 // Copy the code's block-wide tables (check degrees, prior LLRs) to shared memory.
 __device__ __forceinline__ void load_block_tables(const DevGraph& g, const DevArgs& a, unsigned char* smem) {
   uint8_t* s_chk_deg = smem + a.off_chk_deg;
@@ -410,6 +491,8 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
   long long* red = reinterpret_cast<long long*>(gsm + a.g_red);
   volatile long long* shot_slot = red + nwarps;
   const A beta = A(a.beta);
+  const bool first_from_table = MAXDC > 0 && a.first_table && a.llr_shot == nullptr;
+  const M* first_tab = reinterpret_cast<const M*>(smem + a.off_first);
 
   A post[VPT];
   A gam[VPT];
@@ -519,9 +602,11 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
           const int v = t + k * G;
           if (v < V) {
             gam[k] = grow ? A(__ldg(grow + v)) : A(gs);
-            const M m0 = IO::st(llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]));
+            if (!first_from_table) {  // the first check pass reads mu = llr; the table stands in for it
+              const M m0 = IO::st(llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]));
 #pragma unroll
-            for (int j = 0; j < MAXDV; ++j) msg[vpos[k][j]] = m0;
+              for (int j = 0; j < MAXDV; ++j) msg[vpos[k][j]] = m0;
+            }
           }
         }
         group_sync(bar, G);
@@ -578,6 +663,16 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               // and padded to MAXDC: NQ vector loads/stores, padding masked by selects.
               constexpr int NQ = MAXDC / VecIO<M>::N;
               constexpr int VEC = VecIO<M>::N;
+              if (it == 0 && first_from_table) {
+                // first pass of the phase: the block's table row, negated when s = 1
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                  uint4 w = *reinterpret_cast<const uint4*>(first_tab + chunk_base<M>(q, c, C));
+                  if (s) w = flip_signs<M>(w);
+                  *reinterpret_cast<uint4*>(msg + chunk_base<M>(q, c, C)) = w;
+                }
+                continue;
+              }
               const int deg = s_chk_deg[c];
               const int swz = chunk_swizzle<M>(c);
               A mv[MAXDC];
@@ -832,6 +927,7 @@ relaybp_decode_kernel(DevGraph g, DevArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   load_block_tables(g, a, smem);
   __syncthreads();
+  if (a.first_table) build_first_pass_table<M, MAXDC>(g, a, smem);
   run_groups<M, MAXDC, VPT, MAXDV>(g, a, smem);
 }
 
@@ -865,6 +961,7 @@ relaybp_mixed_kernel(const __grid_constant__ MixedArgs m) {
     const DevArgs a = m.code[code].a;
     load_block_tables(g, a, smem);
     __syncthreads();
+    if (a.first_table) build_first_pass_table<M, MAXDC>(g, a, smem);
     run_groups<M, MAXDC, VPT, MAXDV>(g, a, smem);
     __syncthreads();
     if (threadIdx.x == 0) {
