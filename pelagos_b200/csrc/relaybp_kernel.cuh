@@ -609,7 +609,10 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
             }
           }
         }
-        group_sync(bar, G);
+        // The first check pass must see the initial messages.  The table path
+        // writes none here, and the previous phase's (or shot's) last reads of
+        // the messages and hard bytes ended at a group barrier.
+        if (!first_from_table) group_sync(bar, G);
         int valid = 0;
         bool frozen = false;
         for (int it = 0; it <= max_iter; ++it) {
@@ -785,7 +788,9 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               iters += it;
               hard_src = HARD_BEST;
               frozen = true;
-              group_sync(bar, G);  // best_bits and red settled before reuse
+              // No barrier here: each warp's best_bits words are written by that
+              // warp alone and read only after a later barrier, and `red` is
+              // rewritten no sooner than the next phase's check-pass barrier.
               break;
             }
           }
