@@ -41,7 +41,6 @@ struct rbp_decoder {
   int rows = 0;                // check slots per row in the layout (padded, multiple of VEC)
   DevBuf<uint16_t> var_pos;    // [vslots, V] slot index of variable v's k-th edge
   DevBuf<float> llr;
-  DevBuf<long long> wunits;
   DevBuf<float> gamma_legs;
   DevBuf<float> alpha;
   DevBuf<int> queue;
@@ -60,7 +59,7 @@ size_t msg_size(int t) { return t == RBP_MSG_F64 ? 8 : (t == RBP_MSG_F32 ? 4 : 2
 
 struct Layout {
   int off_chk_deg, off_llr, off_first, off_group0;
-  int g_msg, g_hard, g_best, g_first, g_red, group_bytes;
+  int g_msg, g_par, g_best, g_first, g_red, group_bytes;
 };
 
 // Rows of the check-slot layout: the slot count the kernel holds in registers
@@ -96,8 +95,8 @@ Layout make_layout(int C, int V, int rows, int msg_type, int group_threads) {
   int q = 0;
   L.g_msg = q;
   q = align16(q + (int)msg_size(msg_type) * slots_total);
-  L.g_hard = q;
-  q = align16(q + slots_total);
+  L.g_par = q;
+  q = align16(q + 4 * ((C + 31) / 32));
   L.g_best = q;
   q = align16(q + 4 * W);
   L.g_first = q;
@@ -216,7 +215,7 @@ int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outpu
 
 // Fill the kernel arguments and launch (memset of the work counter + kernel) on `st`.
 int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, const Launch& lc, const float* llr,
-                  const long long* wunits, const float* gamma_legs, const float* alpha, int* queue, int64_t B,
+                  const float* gamma_legs, const float* alpha, int* queue, int64_t B,
                   const rbp_batch* in, const rbp_outputs* out, cudaStream_t st, const char* who) {
   DevArgs a{};
   a.pre_iter = in->pre_iter;
@@ -231,7 +230,6 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.beta = p.beta;
   a.gamma0 = in->gamma0;
   a.llr = llr;
-  a.wunits = wunits;
   a.gamma_legs = gamma_legs;
   a.alpha = alpha;
   a.B = B;
@@ -270,7 +268,7 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.off_group0 = L.off_group0;
   a.group_bytes = L.group_bytes;
   a.g_msg = L.g_msg;
-  a.g_hard = L.g_hard;
+  a.g_par = L.g_par;
   a.g_best = L.g_best;
   a.g_first = L.g_first;
   a.g_red = L.g_red;
@@ -468,13 +466,8 @@ int rbp_decoder_create(const rbp_graph* g, const rbp_params* p, const float* llr
 int rbp_decoder_set_llr(rbp_decoder* d, const float* llr) {
   if (!d || !llr) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_set_llr: null argument");
   const int V = d->g->V;
-  std::vector<long long> w(V);
-  for (int v = 0; v < V; ++v)
-    w[v] = std::isfinite(llr[v]) ? (long long)std::llrint(std::ldexp((double)llr[v], 32)) : 0;
   DeviceGuard dg(d->g->device);
-  int rc;
-  if ((rc = d->llr.upload(llr, V)) || (rc = d->wunits.upload(w.data(), V))) return rc;
-  return RBP_OK;
+  return d->llr.upload(llr, V);
 }
 
 int rbp_decoder_destroy(rbp_decoder* d) {
@@ -517,7 +510,7 @@ int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs
   const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, d->group_threads);
   const DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
   const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks};
-  return launch_decode(dgph, d->p, L, lc, d->llr.p, d->wunits.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
+  return launch_decode(dgph, d->p, L, lc, d->llr.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
                        out, reinterpret_cast<cudaStream_t>(stream), "rbp_decode");
 }
 
@@ -575,7 +568,6 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.beta = p.beta;
     a.gamma0 = in->gamma0;
     a.llr = d->llr.p;
-    a.wunits = d->wunits.p;
     a.gamma_legs = d->gamma_legs.p;
     a.alpha = d->alpha.p;
     a.B = B[i];
@@ -614,7 +606,7 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.off_group0 = L.off_group0;
     a.group_bytes = L.group_bytes;
     a.g_msg = L.g_msg;
-    a.g_hard = L.g_hard;
+    a.g_par = L.g_par;
     a.g_best = L.g_best;
     a.g_first = L.g_first;
     a.g_red = L.g_red;
@@ -895,7 +887,7 @@ int rbp_decode_static(int32_t C, int32_t V, int32_t E, const int32_t* chk_ptr, c
   const Layout L = make_layout(C, V, rows, p->msg_type, G);
   const DevGraph dgph{C, V, E, slots, rows, vslots, scratch + off_deg, reinterpret_cast<const int*>(scratch + off_ptr),
                       reinterpret_cast<const uint16_t*>(scratch + off_pos)};
-  return launch_decode(dgph, *p, L, lc, llr, nullptr, gamma_legs, alpha, reinterpret_cast<int*>(scratch), B, in, out,
+  return launch_decode(dgph, *p, L, lc, llr, gamma_legs, alpha, reinterpret_cast<int*>(scratch), B, in, out,
                        st, who);
 }
 

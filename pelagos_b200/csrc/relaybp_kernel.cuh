@@ -16,8 +16,8 @@
 // c = t + k*G (k < ceil(C/G)).  Everything per variable stays in that thread's
 // registers for the whole kernel: the slot positions of its edges (loaded once
 // per kernel), its posterior (carried across legs: the memory), and the leg's
-// memory strength.  Shared memory per group holds only the edge messages, a
-// per-edge copy of the variable's hard decision, and two bit sets.
+// memory strength.  Shared memory per group holds only the edge messages, one
+// parity bit per check, and two bit sets.
 //
 //   msg[rows * C + 1]  edge messages; the slots of check c sit in 16-byte
 //                    chunks (see slot_index), so a check pass moves a row with
@@ -25,19 +25,20 @@
 //                    (no bank conflicts).  A slot holds mu after a variable pass
 //                    and nu after a check pass.  The last slot is a dummy that
 //                    absent variable edges point at.
-//   hard[rows * C + 1] hard decision of the edge's variable, written by the
-//                    variable pass, read by the next check pass (same index).
+//   par[ceil(C/32)]  parity of each check's current hard decisions.  Every
+//                    hard decision starts at 0 with a shot; when the variable
+//                    pass flips one it XORs (shared atomic) the bits of that
+//                    variable's checks, so the bit equals the check's parity.
 //   best[W], first[W] bit sets (W = ceil(V/32)): best solution, first-leg hard
 //                    decision.
 //
 // Iteration t of a phase (reference: decoder.py:2610-2875):
 //   check pass    (c2v min-sum, kernels.py:1052-1215) + parity of iteration t-1
 //   variable pass (v2c + memory mix + posterior + hard, kernels.py:1220-1350)
-// The parity / selection / freeze of iteration t-1 (kernels.py:510-847) is
-// fused into the check pass of iteration t: each check XORs the hard bytes of
-// its row and a barrier reduction (bar.red.and) tells the whole group whether
-// all checks hold.  The nu such a pass writes after a converged iteration is
-// never read: messages restart at every leg.
+// The parity / selection / freeze of iteration t-1 (kernels.py:510-847) comes
+// before the check pass of iteration t: each check compares its parity bit with
+// its syndrome bit and a barrier reduction (bar.red.and) tells the whole group
+// whether all checks hold; the min-sum pass runs only if one fails.
 //
 // Numerics follow the reference kernels operation by operation with one
 // rounding per operation (explicit _rn intrinsics; built with --fmad=false);
@@ -164,7 +165,6 @@ struct DevArgs {
   float beta, gamma0;
   // tables
   const float* llr;              // [V]
-  const long long* wunits;       // [V], or null: units computed from llr
   const float* gamma_legs;       // [num_sets, V]
   const float* alpha;            // [n_alpha]
   // batch inputs
@@ -204,7 +204,7 @@ struct DevArgs {
   // shared-memory layout (byte offsets)
   int off_chk_deg, off_llr, off_first, off_group0, group_bytes;
   int first_table;               // 1: take each phase's first check pass from the block's table
-  int g_msg, g_hard, g_best, g_first, g_red;
+  int g_msg, g_par, g_best, g_first, g_red;
 };
 
 enum HardSrc { HARD_ZERO = 0, HARD_POST = 1, HARD_BEST = 2 };
@@ -228,7 +228,7 @@ constexpr uint16_t kNoSlot = 0xFFFFu;
 // variable pass, whose warps touch the same slot of ~32 consecutive checks,
 // spreads those accesses over all 32 banks instead of 8.  The check pass's
 // work is symmetric in the slots of a row; it only needs the swizzle to know
-// which positions are padding.  The per-edge hard bytes use the same index.
+// which positions are padding.  A slot's check is (index mod VEC*C) / VEC.
 template <typename M>
 __host__ __device__ __forceinline__ int chunk_swizzle(int c) {
   constexpr int VEC = 16 / (int)sizeof(M);
@@ -253,8 +253,7 @@ __host__ __device__ __forceinline__ int chunk_base(int q, int c, int C) {
 }
 
 // 16-byte vector access to VEC consecutive slots, converted to/from the
-// accumulation type; hard_word folds the chunk's hard bytes (0/1 each, the
-// first `valid` of them real) into a word whose popcount parity is theirs.
+// accumulation type.
 template <typename M>
 struct VecIO;
 template <>
@@ -267,12 +266,6 @@ struct VecIO<float> {
   static __device__ __forceinline__ void store(float* p, const float* o) {
     *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
   }
-  // Hard bytes of a chunk in logical slot order (XOR swizzle undone), the
-  // first `valid` kept: a word whose popcount parity is the chunk's parity.
-  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid, int swz) {
-    const uint32_t w = __byte_perm(*reinterpret_cast<const uint32_t*>(p), 0u, 0x3210u ^ (0x1111u * swz));
-    return valid >= 4 ? w : (valid <= 0 ? 0u : w & ((1u << (8 * valid)) - 1u));
-  }
 };
 template <>
 struct VecIO<double> {
@@ -283,11 +276,6 @@ struct VecIO<double> {
   }
   static __device__ __forceinline__ void store(double* p, const double* o) {
     *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
-  }
-  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid, int swz) {
-    uint32_t w = *reinterpret_cast<const uint16_t*>(p);
-    if (swz) w = ((w & 0xFFu) << 8) | (w >> 8);
-    return valid >= 2 ? w : (valid <= 0 ? 0u : w & 0xFFu);
   }
 };
 template <typename H, float (*ToF)(H), H (*FromF)(float), unsigned short (*Bits)(H), H (*FromBits)(unsigned short)>
@@ -308,16 +296,6 @@ struct VecIO16 {
     for (int i = 0; i < 4; ++i)
       w[i] = (uint32_t)Bits(FromF(o[2 * i])) | ((uint32_t)Bits(FromF(o[2 * i + 1])) << 16);
     *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
-  }
-  static __device__ __forceinline__ uint32_t hard_word(const uint8_t* p, int valid, int swz) {
-    const uint2 raw = *reinterpret_cast<const uint2*>(p);
-    const uint32_t sel = 0x3210u ^ (0x1111u * (swz & 2));
-    const uint32_t w0 = __byte_perm((swz & 4) ? raw.y : raw.x, 0u, sel);
-    const uint32_t w1 = __byte_perm((swz & 4) ? raw.x : raw.y, 0u, sel);
-    const uint32_t lo = valid >= 4 ? w0 : (valid <= 0 ? 0u : w0 & ((1u << (8 * valid)) - 1u));
-    const int v2 = valid - 4;
-    const uint32_t hi = v2 >= 4 ? w1 : (v2 <= 0 ? 0u : w1 & ((1u << (8 * v2)) - 1u));
-    return lo ^ hi;
   }
 };
 __device__ __forceinline__ float h2f(__half h) { return __half2float(h); }
@@ -485,7 +463,10 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
 
   unsigned char* gsm = smem + a.off_group0 + gid * a.group_bytes;
   M* msg = reinterpret_cast<M*>(gsm + a.g_msg);
-  uint8_t* hard = gsm + a.g_hard;
+  // parity of each check's current hard decisions, bit c%32 of word c/32
+  uint32_t* par_bits = reinterpret_cast<uint32_t*>(gsm + a.g_par);
+  const int Wc = (C + 31) >> 5;
+  const int VC = VecIO<M>::N * C;  // elements per chunk column: slot p belongs to check (p % VC) / VEC
   uint32_t* best_bits = reinterpret_cast<uint32_t*>(gsm + a.g_best);
   uint32_t* first_bits = reinterpret_cast<uint32_t*>(gsm + a.g_first);
   long long* red = reinterpret_cast<long long*>(gsm + a.g_red);
@@ -524,6 +505,10 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
       for (int c = t; c < C; c += G, ++k) synm |= (uint32_t)(syn_row[c] & 1) << k;
     }
     const float* llr_row = a.llr_shot ? a.llr_shot + b * (long long)V : nullptr;
+    // every hard decision starts at 0 (parity 0 for every check); the first variable pass
+    // flips the ones it sets
+    for (int w = t; w < Wc; w += G) par_bits[w] = 0u;
+    uint32_t hmask = 0;  // bit k: hard decision of variable t + k*G
     long long best_w = LLONG_MAX;
     int found = 0, iters = 0, hard_src = HARD_ZERO, sought = 1;
     bool has_best = false;
@@ -601,7 +586,8 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         for (int k = 0; k < VPT; ++k) {
           const int v = t + k * G;
           if (v < V) {
-            gam[k] = grow ? A(__ldg(grow + v)) : A(gs);
+            gam[k] = A(gs);
+            if (grow) gam[k] = A(__ldg(grow + v));  // first read in the variable pass
             if (!first_from_table) {  // the first check pass reads mu = llr; the table stands in for it
               const M m0 = IO::st(llr_row ? A(__ldg(llr_row + v)) : A(s_llr[v]));
 #pragma unroll
@@ -611,7 +597,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         }
         // The first check pass must see the initial messages.  The table path
         // writes none here, and the previous phase's (or shot's) last reads of
-        // the messages and hard bytes ended at a group barrier.
+        // the messages and parity bits ended at a group barrier.
         if (!first_from_table) group_sync(bar, G);
         int valid = 0;
         bool frozen = false;
@@ -630,23 +616,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
             int kp = 0;
             for (int c = t; c < C; c += G, ++kp) {
               const int s = (int)((synm >> kp) & 1u);
-              int par;
-              if constexpr (MAXDC > 0) {
-                constexpr int NQ = MAXDC / VecIO<M>::N;
-                constexpr int VEC = VecIO<M>::N;
-                const int deg = s_chk_deg[c];
-                const int swz = chunk_swizzle<M>(c);
-                uint32_t x = 0;
-#pragma unroll
-                for (int q = 0; q < NQ; ++q)
-                  x ^= VecIO<M>::hard_word(hard + chunk_base<M>(q, c, C), deg - q * VEC, swz);
-                par = __popc(x) & 1;
-              } else {
-                const int deg = g.chk_ptr[c + 1] - g.chk_ptr[c];
-                int hp = 0;
-                for (int j = 0; j < deg; ++j) hp ^= hard[slot_index<M>(j, c, C)];
-                par = hp & 1;
-              }
+              const int par = (int)((par_bits[c >> 5] >> (c & 31)) & 1u);
               okp = okp && (par == s);
             }
             all_ok = group_all(bar, G, okp);
@@ -659,7 +629,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
           int k = 0;
           for (int c = t; c < C; c += G, ++k) {
             const int s = (int)((synm >> k) & 1u);
-            int hp = 0, neg = 0, cnt1 = 0;
+            int neg = 0, cnt1 = 0;
             A min1 = A(1e30), min2 = A(1e30);
             if constexpr (MAXDC > 0) {
               // The row's slots are contiguous in 16-byte chunks (VEC messages each)
@@ -682,13 +652,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
 #pragma unroll
               for (int q = 0; q < NQ; ++q)
                 VecIO<M>::load(msg + chunk_base<M>(q, c, C), mv + q * VecIO<M>::N);
-              if (chk_par) {
-                uint32_t x = 0;
-#pragma unroll
-                for (int q = 0; q < NQ; ++q)
-                  x ^= VecIO<M>::hard_word(hard + chunk_base<M>(q, c, C), deg - q * VEC, swz);
-                ok_all = ok_all && ((__popc(x) & 1) == s);
-              }
+              if (chk_par) ok_all = ok_all && ((int)((par_bits[c >> 5] >> (c & 31)) & 1u) == s);
               if (write_nu) {
                 // min1 = min(1e30, |mu_j|), min2 = the second smallest (a tie gives
                 // min2 == min1): the argmin edge receives min2 exactly when it is
@@ -732,14 +696,13 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               for (int j = 0; j < deg; ++j) {
                 const int ix = slot_index<M>(j, c, C);
                 const A m = IO::ld(msg[ix]);
-                if (chk_par) hp ^= hard[ix];
                 neg ^= (m < A(0)) ? 1 : 0;
                 const A x = fabs(m);
                 if (x < min1) { min2 = min1; min1 = x; cnt1 = 1; }
                 else if (x == min1) { cnt1 += 1; }
                 else if (x < min2) { min2 = x; }
               }
-              if (chk_par) ok_all = ok_all && ((hp & 1) == s);
+              if (chk_par) ok_all = ok_all && ((int)((par_bits[c >> 5] >> (c & 31)) & 1u) == s);
               if (write_nu) {
                 const bool par = ((neg ^ s) & 1) != 0;
                 for (int j = 0; j < deg; ++j) {
@@ -766,15 +729,14 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               for (int kk = 0; kk < VPT; ++kk) {
                 const int v = t + kk * G;
                 if (v < V && post[kk] <= A(0))
-                  w += llr_row ? weight_units(__ldg(llr_row + v))
-                               : (a.wunits ? __ldg(a.wunits + v) : weight_units(s_llr[v]));
+                  w += weight_units(llr_row ? __ldg(llr_row + v) : s_llr[v]);
               }
 #pragma unroll
               for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-              if (lane == 0) red[warp] = w;
+              // red[0] was cleared by this phase's variable pass (before its barrier)
+              if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long*>(red), (unsigned long long)w);
               group_sync(bar, G);
-              long long tot = 0;
-              for (int i = 0; i < nwarps; ++i) tot += red[i];
+              const long long tot = red[0];
               if (!has_best || tot < best_w) {
                 best_w = tot;
                 has_best = true;
@@ -814,16 +776,34 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
               }
               const A pv = add_rn(lm, sum);
               post[kk] = pv;
-              const uint8_t h = pv <= A(0) ? 1 : 0;
 #pragma unroll
               for (int j = 0; j < MAXDV; ++j) {
                 const uint32_t p = vpos[kk][j];
                 msg[p] = IO::st(add_rn(lm, sub_rn(sum, nv[j])));
-                hard[p] = h;
+              }
+              const uint32_t h = pv <= A(0) ? 1u : 0u;
+              if (h != ((hmask >> kk) & 1u)) {
+                // the decision flipped: so does the parity of each of its checks
+                hmask ^= 1u << kk;
+#pragma unroll
+                for (int j = 0; j < MAXDV; ++j) {
+                  uint32_t q = vpos[kk][j];
+                  if (q != dummy) {
+                    if constexpr (MAXDC > 0) {
+#pragma unroll
+                      for (int r = 1; r < MAXDC / VecIO<M>::N; ++r) q = q >= (uint32_t)VC ? q - (uint32_t)VC : q;
+                    } else {
+                      while (q >= (uint32_t)VC) q -= (uint32_t)VC;
+                    }
+                    const uint32_t c = q / (uint32_t)VecIO<M>::N;
+                    atomicXor(par_bits + (c >> 5), 1u << (c & 31u));
+                  }
+                }
               }
             }
           }
           hard_src = HARD_POST;
+          if (t == 0) red[0] = 0;  // the next selection's sum; its last reader passed a barrier since
           group_sync(bar, G);
         }
         if (!frozen) iters += max_iter;
