@@ -478,9 +478,11 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
   A post[VPT];
   A gam[VPT];
 
+  int q_early = -1;  // thread 0: the queue position claimed while the last shot wrote its outputs
   while (true) {
     if (t == 0) {
-      const long long q = (long long)atomicAdd(a.queue, 1);
+      const long long q = (long long)(q_early >= 0 ? q_early : atomicAdd(a.queue, 1));
+      q_early = -1;
       const long long qn = a.queue_len ? (long long)max(0, min(*a.queue_len, (int)a.B)) : a.B;
       long long sb = q < qn ? q : a.B;
       if (q < qn && a.order) {
@@ -498,34 +500,27 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
     }
 
     // ---------------- per-shot setup (decoder.py:3429-3478)
+    // Every load of the shot's inputs is issued before any of them is used, so the
+    // latencies of the saved state and the syndrome overlap.
     const uint8_t* syn_row = a.syn + b * (long long)C;
-    uint32_t synm = 0;  // bit k: syndrome of check t + k*G
-    {
-      int k = 0;
-      for (int c = t; c < C; c += G, ++k) synm |= (uint32_t)(syn_row[c] & 1) << k;
-    }
     const float* llr_row = a.llr_shot ? a.llr_shot + b * (long long)V : nullptr;
-    // every hard decision starts at 0 (parity 0 for every check); the first variable pass
-    // flips the ones it sets
-    for (int w = t; w < Wc; w += G) par_bits[w] = 0u;
-    uint32_t hmask = 0;  // bit k: hard decision of variable t + k*G
     long long best_w = LLONG_MAX;
-    int found = 0, iters = 0, hard_src = HARD_ZERO, sought = 1;
-    bool has_best = false;
+    int found = 0, iters = 0, hard_src = HARD_ZERO, sought = 1, has_best_raw = 0;
     const int pre = a.pre_iter;
-    if (a.resume) {
+    const unsigned char* st = a.resume ? a.resume + b * (long long)a.state_stride : nullptr;
+    const uint32_t* st_bits = st ? reinterpret_cast<const uint32_t*>(st + 32) : nullptr;
+    uint32_t bits0 = 0u, bits1 = 0u;  // this thread's first words of the two saved bit sets
+    if (st) {
       // continue a shot suspended after an earlier phase
-      const unsigned char* st = a.resume + b * (long long)a.state_stride;
       const int* hdr = reinterpret_cast<const int*>(st);
       found = hdr[0];
       iters = hdr[1];
       hard_src = hdr[2];
-      has_best = hdr[3] != 0;
+      has_best_raw = hdr[3];
       best_w = *reinterpret_cast<const long long*>(st + 16);
-      const uint32_t* bits = reinterpret_cast<const uint32_t*>(st + 32);
-      for (int w = t; w < W; w += G) {
-        best_bits[w] = bits[w];
-        first_bits[w] = bits[W + w];
+      if (t < W) {
+        bits0 = st_bits[t];
+        bits1 = st_bits[W + t];
       }
       const A* sp = reinterpret_cast<const A*>(st + state_post_offset(V));
 #pragma unroll
@@ -544,6 +539,30 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
         }
         post[k] = p0;
       }
+    }
+    uint32_t synm = 0;  // bit k: syndrome of check t + k*G; four loads in flight per round
+    for (int k = 0, c = t; c < C; k += 4, c += 4 * G) {
+      const uint32_t s0 = syn_row[c];
+      const uint32_t s1 = c + G < C ? (uint32_t)syn_row[c + G] : 0u;
+      const uint32_t s2 = c + 2 * G < C ? (uint32_t)syn_row[c + 2 * G] : 0u;
+      const uint32_t s3 = c + 3 * G < C ? (uint32_t)syn_row[c + 3 * G] : 0u;
+      synm |= ((s0 & 1u) | ((s1 & 1u) << 1) | ((s2 & 1u) << 2) | ((s3 & 1u) << 3)) << k;
+    }
+    // every hard decision starts at 0 (parity 0 for every check); the first variable pass
+    // flips the ones it sets
+    for (int w = t; w < Wc; w += G) par_bits[w] = 0u;
+    uint32_t hmask = 0;  // bit k: hard decision of variable t + k*G
+    bool has_best = has_best_raw != 0;
+    if (st) {
+      if (t < W) {
+        best_bits[t] = bits0;
+        first_bits[t] = bits1;
+      }
+      for (int w = t + G; w < W; w += G) {
+        best_bits[w] = st_bits[w];
+        first_bits[w] = st_bits[W + w];
+      }
+    } else {
       for (int w = t; w < W; w += G) {
         best_bits[w] = 0u;
         first_bits[w] = 0u;
@@ -832,6 +851,7 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
 
     // ---------------- outputs, decoder.py:3839-3873
     group_sync(bar, G);
+    if (t == 0) q_early = atomicAdd(a.queue, 1);
     if (a.suspend && (!a.suspend_unsolved || stopped_unsolved)) {
       unsigned char* st = a.suspend + b * (long long)a.state_stride;
       if (t == 0) {
