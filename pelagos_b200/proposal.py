@@ -29,7 +29,7 @@ import json
 import time
 from dataclasses import asdict, dataclass
 from pathlib import Path
-from typing import Dict, Optional
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -258,6 +258,10 @@ class LearnedRelayBPDecoder:
     the syndromes into the captured input buffer and replays the graph.  Calls
     that pass ``events`` run eagerly.  Not for concurrent use from several
     streams: the buffers and graphs belong to the decoder object.
+
+    ``decode_stream(batches)`` decodes a sequence of host batches with the
+    host/device copies overlapped with the decodes (two sets of buffers and
+    graphs, a copy stream).
     """
 
     def __init__(self, decoder: RelayBPDecoder, net: ProposalNet, learned_legs: int = 4, gate: bool = False,
@@ -272,12 +276,15 @@ class LearnedRelayBPDecoder:
         self.gate = bool(gate)
         self.fused = bool(fused)
         self.graph = bool(graph)
-        self._graphs: Dict[int, tuple] = {}
-        self._bufs: Dict[int, dict] = {}
+        self._graphs: Dict[tuple, tuple] = {}  # (B, slot) -> (graph, static input, buffers)
+        self._bufs: Dict[tuple, dict] = {}     # (B, slot) -> buffers
+        self._copy_stream: Optional[torch.cuda.Stream] = None
 
-    def _buffers(self, B: int) -> dict:
-        b = self._bufs.get(B)
+    def _buffers(self, B: int, slot: int = 0) -> dict:
+        b = self._bufs.get((B, slot))
         if b is None:
+            if any(k[0] != B for k in self._bufs):
+                self._bufs, self._graphs = {}, {}  # keep one batch size; graphs refer to their buffers
             d, dev = self.dec, self.net.device
             b = {
                 "state": d.new_state(B),
@@ -288,36 +295,40 @@ class LearnedRelayBPDecoder:
                 "errors": torch.empty(B, d.V, dtype=torch.uint8, device=dev),
                 "count": torch.empty(1, dtype=torch.int32, device=dev),
             }
-            self._bufs = {B: b}  # keep one batch size
-            self._graphs = {}    # captured graphs refer to the buffers they were captured with
+            self._bufs[(B, slot)] = b
         return b
 
-    def _replay(self, syn: torch.Tensor) -> dict:
-        """Copy the syndromes (host or device) into the captured input buffer and replay."""
+    def _graph_entry(self, syn: torch.Tensor, slot: int = 0) -> tuple:
+        """(graph, static input, buffers) of this batch size and buffer set; captured on first
+        use from an eager warm-up decode of ``syn``."""
         B = int(syn.shape[0])
-        entry = self._graphs.get(B)
+        entry = self._graphs.get((B, slot))
         if entry is None:
             static = torch.empty(B, self.dec.C, dtype=torch.uint8, device=self.net.device)
             static.copy_(syn)
-            self.decode_into(static)  # eager warm-up: buffers, kernel attributes, allocator pool
+            self.decode_into(static, slot=slot)  # eager warm-up: buffers, kernel attributes, allocator pool
             torch.cuda.synchronize(self.net.device)
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
-                bf = self.decode_into(static)
+                bf = self.decode_into(static, slot=slot)
             entry = (g, static, bf)
-            self._graphs[B] = entry
-        g, static, bf = entry
+            self._graphs[(B, slot)] = entry
+        return entry
+
+    def _replay(self, syn: torch.Tensor) -> dict:
+        """Copy the syndromes (host or device) into the captured input buffer and replay."""
+        g, static, bf = self._graph_entry(syn)
         static.copy_(syn, non_blocking=True)
         g.replay()
         return bf
 
-    def decode_into(self, syn: torch.Tensor, events=None) -> dict:
+    def decode_into(self, syn: torch.Tensor, events=None, slot: int = 0) -> dict:
         """Launch the three phases into the persistent buffers of this batch size (no host sync).
         ``events``: four CUDA events recorded before the pre-iterations, after them, after the
         network (with its shot selection) and after the relay legs."""
         d = self.dec
         B = int(syn.shape[0])
-        bf = self._buffers(B)
+        bf = self._buffers(B, slot)
         gid = d.device_ids[0]
         stream = torch.cuda.current_stream(self.net.device).cuda_stream
         gamma0 = float(np.float32(d.gamma0))
@@ -422,6 +433,72 @@ class LearnedRelayBPDecoder:
             "unconverged_indices": torch.nonzero(found < d.stop_nconv).flatten().to(torch.int32),
             "weight_fixed": wfix,
         }
+
+    STREAM_KEYS = (("errors", "errors", torch.uint8), ("weight_fixed", "wfix", torch.int64),
+                   ("found_count", "found", torch.int32), ("iterations", "iters", torch.int32))
+
+    def decode_stream(self, batches: Sequence[torch.Tensor],
+                      out: Optional[Sequence[Dict[str, torch.Tensor]]] = None) -> List[Dict[str, torch.Tensor]]:
+        """Decode a sequence of host syndrome batches, all [B, C] uint8 on the CPU (pinned for
+        the copies to overlap), with the transfers hidden behind the decodes.  Two sets of
+        device buffers and captured graphs alternate: while batch i decodes on the current
+        stream, a copy stream brings batch i+1's syndromes in and batch i-1's results out.
+
+        ``out[i]`` (CPU tensors, pinned for overlap; allocated pinned when ``out`` is None)
+        receives batch i's ``errors`` [B, V] uint8, ``weight_fixed`` [B] int64, ``found_count``
+        and ``iterations`` [B] int32 -- the same values ``decode`` returns for that batch.  Entries
+        of ``out`` may repeat (a ring of host buffers); each is written in batch order.  Returns
+        after every copy has finished."""
+        n = len(batches)
+        if n == 0:
+            return []
+        d, dev = self.dec, self.net.device
+        B = int(batches[0].shape[0])
+        for x in batches:
+            if x.device.type != "cpu" or x.dtype != torch.uint8 or tuple(x.shape) != (B, d.C):
+                raise ValueError(f"decode_stream takes CPU uint8 batches of shape [{B}, {d.C}]")
+        if B == 0:
+            raise ValueError("decode_stream needs non-empty batches")
+        if out is None:
+            out = [{k: torch.empty((B, d.V) if k == "errors" else (B,), dtype=t).pin_memory()
+                    for k, _, t in self.STREAM_KEYS} for _ in range(n)]
+        if len(out) != n:
+            raise ValueError("out must hold one entry per batch")
+        entries = [self._graph_entry(batches[0], slot) for slot in range(min(2, n))]
+        compute = torch.cuda.current_stream(dev)
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream(dev)
+        copy = self._copy_stream
+        start = torch.cuda.Event()
+        start.record(compute)
+        copy.wait_event(start)
+        h2d: List[Optional[torch.cuda.Event]] = [None] * n
+
+        def bring_in(i: int) -> None:
+            # on the copy stream after batch i-2's results left the same buffers
+            with torch.cuda.stream(copy):
+                entries[i % 2][1].copy_(batches[i], non_blocking=True)
+                h2d[i] = torch.cuda.Event()
+                h2d[i].record(copy)
+
+        bring_in(0)
+        for i in range(n):
+            g, _, bf = entries[i % 2]
+            compute.wait_event(h2d[i])
+            g.replay()
+            decoded = torch.cuda.Event()
+            decoded.record(compute)
+            if i + 1 < n:
+                bring_in(i + 1)
+            with torch.cuda.stream(copy):
+                copy.wait_event(decoded)
+                for key, buf, _ in self.STREAM_KEYS:
+                    out[i][key].copy_(bf[buf], non_blocking=True)
+        finished = torch.cuda.Event()
+        finished.record(copy)
+        compute.wait_event(finished)  # work queued after this call sees the results in place
+        finished.synchronize()
+        return list(out)
 
 
 def default_weights_path(workload: str = "bb144_phen", p: float = 0.003) -> Path:

@@ -176,6 +176,30 @@ def test_graph_replay_equals_eager(setup):
             np.testing.assert_array_equal(a[k], b[k], err_msg=k)
 
 
+def test_decode_stream_equals_decode(setup):
+    """The overlapped stream of host batches returns, batch by batch, what decode() returns,
+    into a ring of two pinned host buffer sets and into freshly allocated ones."""
+    s = setup
+    w = codes.workload("bb144_phen", p=0.005)
+    dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    net = ProposalNet(dec, s["theta"])
+    learned = LearnedRelayBPDecoder(dec, net, gate=True)
+    batches = [torch.from_numpy(w.sample(2048, seed=40 + i)[1]).pin_memory() for i in range(5)]
+    ref = [{k: v.cpu().numpy() for k, v in learned.decode(b).items()} for b in batches]
+    keys = ("errors", "weight_fixed", "found_count", "iterations")
+    got = learned.decode_stream(batches)
+    for i in range(5):
+        for k in keys:
+            np.testing.assert_array_equal(got[i][k].numpy(), ref[i][k], err_msg=f"{k} of batch {i}")
+    ring = [{k: torch.empty_like(v).pin_memory() for k, v in got[0].items()} for _ in range(2)]
+    for i in range(5):
+        out = learned.decode_stream(batches[: i + 1], out=[ring[j % 2] for j in range(i + 1)])
+        for k in keys:
+            np.testing.assert_array_equal(out[i][k].numpy(), ref[i][k], err_msg=f"{k} of batch {i} (ring)")
+    with pytest.raises(ValueError):
+        learned.decode_stream([batches[0].to(DEV)])
+
+
 def test_training_lowers_the_loss(setup):
     s = setup
     cfg = TrainConfig(tuples=96 * 256, batch=256, lr=3e-3, lr_final=1e-3, log_every=32, seed=11)
