@@ -130,6 +130,21 @@ __device__ __forceinline__ void group_sync(int id, int n) {
   }
 }
 
+// Barrier + OR-reduction of a predicate over the group.
+__device__ __forceinline__ bool group_any(int id, int n, bool p) {
+  if (n == 32) return __any_sync(0xffffffffu, p);
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "bar.red.or.pred po, %2, %3, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)p), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+
 // Barrier + AND-reduction of a predicate over the group.
 __device__ __forceinline__ bool group_all(int id, int n, bool p) {
   if (n == 32) return __all_sync(0xffffffffu, p);
@@ -552,6 +567,8 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
     // flips the ones it sets
     for (int w = t; w < Wc; w += G) par_bits[w] = 0u;
     uint32_t hmask = 0;  // bit k: hard decision of variable t + k*G
+    uint32_t hmask_sel = 0;   // this thread's decisions at the shot's last computed selection
+    bool sel_seen = false;    // a selection has been computed for this shot (group-uniform)
     bool has_best = has_best_raw != 0;
     if (st) {
       if (t < W) {
@@ -742,7 +759,14 @@ __device__ __forceinline__ void run_groups(const DevGraph& g, const DevArgs& a, 
 
           if (check_parity) {
             // check_and_select_kernel (kernels.py:609-741) for iteration it-1
-            if (all_ok) {
+            // the decisions of the last computed selection again: same weight, best unchanged
+            const bool repeat = all_ok && sel_seen && !group_any(bar, G, hmask != hmask_sel);
+            if (repeat) {
+              if (valid == 0) found += 1;
+              valid = 1;
+            } else if (all_ok) {
+              hmask_sel = hmask;
+              sel_seen = true;
               long long w = 0;
 #pragma unroll
               for (int kk = 0; kk < VPT; ++kk) {
