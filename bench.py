@@ -337,7 +337,7 @@ def main():
     e2e_value = whole_job_shots_per_s(world, shots, e2e_ms)
     # (b) one decode() call per batch, its results copied to pinned host memory before the next
     res_pin = ring[0]
-    call_steps = max(1, min(args.steps, 3))
+    call_steps = max(1, min(args.steps, 10))
     barrier()
     c0, c1 = ev(), ev()
     c0.record(stream)
