@@ -23,7 +23,15 @@ run and is reported under "plain", with both logical error rates.
          batch with its copies in series.
 
 `--impl reference` times the reference algorithm's CPU implementation (the CPU
-oracle: the reference's Rust crate is not available) on the host cores.
+oracle: the reference's Rust crate is not available) on every host core, one
+whole 65,536-shot batch per step, with the leg strengths the GPU arm uses
+(torch's CUDA generator, seeded per leg as the reference draws them).
+
+Roofline: the decode keeps each shot's messages in shared memory, so the bound
+is shared-memory bandwidth (SMs x 128 B/clk x the sampled SM clock); the
+algorithmic bytes per shot-iteration are those of a state-streaming decode
+(16 E + 13 V + 2 C for float32).  The measured DRAM traffic is reported beside
+it with its fraction of the HBM copy bandwidth.
 Multi-GPU runs (torchrun) are independent replicas: each rank decodes its own
 batch (weak scaling, no collective on the data path).
 """
@@ -166,40 +174,66 @@ def cpu_baseline(w, syn, legs, seconds: float = 12.0) -> dict:
             "mean_iterations": float(out["iterations"].mean())}
 
 
+def leg_table_cuda(V: int) -> tuple[np.ndarray, bool]:
+    """The relay legs' strengths as the decoder draws them: leg l from torch's CUDA generator seeded
+    with seed + l (utils.py:128-160), so both arms decode the same trajectories.  Falls back to the
+    CPU generator (another table) only where no GPU is visible."""
+    import torch
+
+    from pelagos_b200.utils import sample_gamma_uniform
+
+    lo, hi = RELAY["gamma_dist_interval"]
+    cuda = torch.cuda.is_available()
+    dev = "cuda:0" if cuda else "cpu"
+    rows = [sample_gamma_uniform(1, V, lo, hi, dev, RELAY["seed"] + leg) for leg in range(RELAY["num_sets"])]
+    return torch.cat(rows).float().cpu().numpy(), cuda
+
+
 def run_reference_arm(args) -> None:
+    """One step = the whole 65,536-shot batch decoded by the CPU oracle on every host core."""
     rank, world, _ = _dist()
     if rank != 0:
         return
+    from oracle import oracle as O
     from pelagos_b200 import codes
 
     w = codes.workload(WORKLOAD, p=P)
     err, syn = w.sample(SHOTS, seed=SEED)
-    # Leg gammas: the decoder draws them with torch's CUDA generator; the CPU arm
-    # uses the same seeded draws computed on the CPU generator.
-    import torch
-
-    lo, hi = RELAY["gamma_dist_interval"]
-    legs = []
-    for leg in range(RELAY["num_sets"]):
-        gen = torch.Generator(device="cpu")
-        gen.manual_seed(RELAY["seed"] + leg)
-        legs.append((lo + (hi - lo) * torch.rand(1, w.H.shape[1], generator=gen)).numpy())
-    legs = np.concatenate(legs).astype(np.float32)
-    per_step = min(args.ref_seconds, 90.0 / max(args.steps, 1))  # whole run within a few minutes
+    legs, same_table = leg_table_cuda(w.H.shape[1])
+    g = O.reference_graph(w.H)
+    llr = O.llr_from_priors(w.priors)
+    threads = O.default_threads()
+    kw = dict(pre_iter=80, num_sets=100, set_max_iter=60, stop_nconv=5, gamma0=0.65, gamma_legs=legs,
+              threads=threads)
     for _ in range(args.warmup):
-        cpu_baseline(w, syn, legs, seconds=1.0)
-    vals = [cpu_baseline(w, syn, legs, seconds=per_step) for _ in range(args.steps)]
-    v = float(np.mean([x["value"] for x in vals]))
-    base = vals[-1]
+        O.decode(g, syn, llr, **kw)
+    times, iters = [], 0.0
+    wall0 = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = O.decode(g, syn, llr, **kw)
+        times.append(time.perf_counter() - t0)
+        iters = float(out["iterations"].mean())
+    wall = time.perf_counter() - wall0
+    ms = 1000.0 * float(np.mean(times))
+    v = SHOTS / (ms / 1000.0)
+    conv = out["found_count"] > 0
+    fails = w.logical_failures(err, out["errors"], conv)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "shots/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * SHOTS / v,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded i.i.d. Bernoulli errors, s = H e mod 2)",
-        "config": {"workload": CONFIG_NAME, "shots": SHOTS, "p": P, "schedule": "pre 80, 100 legs x 60, S=5"},
-        "cpu_baseline": {"value": v, "unit": "shots/s", "cores": base["cores"], "kind": "port",
-                         "sample": base["sample"]},
+        "config": {"workload": CONFIG_NAME, "shots": SHOTS, "p": P, "schedule": "pre 80, 100 legs x 60, S=5",
+                   "leg_strengths": "torch CUDA generator, seed 1234 + leg (the GPU arm's table)"
+                   if same_table else "torch CPU generator (no GPU visible: not the GPU arm's table)"},
+        "cpu_baseline": {"value": v, "unit": "shots/s", "cores": threads, "kind": "port",
+                         "sample": f"the whole {SHOTS}-shot batch per step, full Relay-BP-S schedule, fp32"},
         "e2e": {"value": v, "unit": "shots/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "mean_iterations": iters,
+        "logical_error_rate": {"failures": int(fails.sum()), "shots": SHOTS,
+                               "ci95": list(_wilson(int(fails.sum()), SHOTS))},
+        "same_config": bool(same_table), "timed_wall_s": wall,
         "note": "the reference's CPU implementation is the relay-bp Rust crate (not installable here); "
                 "this arm runs the oracle port of the same algorithm on every host core",
     }
@@ -216,8 +250,10 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shots", type=int, default=SHOTS)
-    ap.add_argument("--launch", default=None, help="G,groups: kernel shape (default: autotuned)")
-    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--launch", default=None,
+                    help="G,groups[,shots_per_group]: kernel shape (default: the committed shape of this workload)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time the candidate shapes on the learned decode (the measured path) first")
     ap.add_argument("--workload", default="bb144_phen", choices=["bb144_phen", "mixed"])
     args = ap.parse_args()
     if args.impl == "reference":
@@ -247,16 +283,21 @@ def main():
     w = codes.workload(WORKLOAD, p=P)
     shots = args.shots
     err, syn = w.sample(shots, seed=SEED + rank)
+    from pelagos_b200 import autotune
+
     launch = tuple(int(x) for x in args.launch.split(",")) if args.launch else None
     dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], launch=launch, **RELAY)
+    if launch is None:
+        shape = autotune.default_shape(dec)  # the shape committed for this workload, if any
+        if shape is not None:
+            dec.configure_launch(*shape)
     params, meta = load_params(default_weights_path(WORKLOAD, P))
     learned = LearnedRelayBPDecoder(dec, ProposalNet(dec, params), learned_legs=LEARNED_LEGS, gate=True)
     syn_dev = torch.from_numpy(syn).to(dev)
     syn_pin = torch.from_numpy(syn).pin_memory()
-    if launch is None and not args.no_autotune:
-        from pelagos_b200 import autotune
-
-        autotune.tune(dec, syn_dev)
+    if launch is None and args.autotune:
+        autotune.tune(dec, syn_dev, decode_fn=lambda s: learned.decode_into(s), repeats=5, use_cache=False,
+                      verbose=rank == 0)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream()
 
@@ -268,34 +309,32 @@ def main():
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    def timed_steps(fn, phases: bool):
-        """K steps bracketed by one pair of events (value); per-step events for the kernel times."""
+    def timed_steps(fn):
+        """K steps, each between its own pair of events on the launching stream; the L2 flush between
+        steps (a 256 MB write) lies outside them.  The region is bracketed by a barrier and a device
+        synchronisation on both sides; ms per step is the mean over steps, max over ranks."""
         for _ in range(args.warmup):
-            fn(None)
+            fn()
             flush.zero_()
         barrier()
-        t_start, t_end = ev(), ev()
-        step_ev = [[ev() for _ in range(4 if phases else 2)] for _ in range(args.steps)]
+        step_ev = [[ev(), ev()] for _ in range(args.steps)]
         step_iters, o = [], None
-        t_start.record(stream)
         for k in range(args.steps):
             flush.zero_()
-            if not phases:
-                step_ev[k][0].record(stream)
-            o = fn(step_ev[k] if phases else None)
-            if not phases:
-                step_ev[k][1].record(stream)
+            step_ev[k][0].record(stream)
+            o = fn()
+            step_ev[k][1].record(stream)
             step_iters.append(o["iterations"])  # only the counts are kept across steps
-        t_end.record(stream)
         barrier()
-        ms = max_over_ranks(t_start.elapsed_time(t_end) / args.steps, pg, dev)
+        per_step = [a.elapsed_time(b) for a, b in step_ev]
+        ms = max_over_ranks(float(np.mean(per_step)), pg, dev)
         iters = sum(int(it.sum().item()) for it in step_iters) / args.steps
-        return ms, step_ev, o, iters
+        return ms, per_step, o, iters
 
     clocks = ClockSampler(local).start()
     wall0 = time.time()
     # ---------------- the learned (gated) decode: the headline (CUDA-graph replay per call)
-    ms_step, _, out, l_iters = timed_steps(lambda e: learned.decode(syn_dev), phases=False)
+    ms_step, l_steps, out, l_iters = timed_steps(lambda: learned.decode(syn_dev))
     # the same decode run eagerly with events between its launches, for the kernel times
     l_ev = []
     for _ in range(3):
@@ -307,7 +346,7 @@ def main():
     decode_ms = [e[0].elapsed_time(e[1]) + e[2].elapsed_time(e[3]) for e in l_ev]
     net_ms = [e[1].elapsed_time(e[2]) for e in l_ev]
     # ---------------- the plain decode of the same shots
-    p_ms, p_ev, p_out, p_iters = timed_steps(lambda e: dec.decode(syn_dev), phases=False)
+    p_ms, p_steps, p_out, p_iters = timed_steps(lambda: dec.decode(syn_dev))
     wall1 = time.time()
     clocks.stop()
     value = whole_job_shots_per_s(world, shots, ms_step)
@@ -362,12 +401,15 @@ def main():
         bps = algorithmic_bytes_per_shot_iteration(w.H.shape[0], V, w.H.nnz,
                                                    {"float32": 4, "float64": 8}.get(args.dtype, 2))
         kern = float(np.mean(decode_ms))
-        achieved = bps * l_iters / (kern / 1000.0) / 1e9  # the two decode launches of a step
+        achieved = bps * l_iters / (kern / 1000.0) / 1e9  # GB/s over the two decode launches of a step
         peaks = _peaks()
         clk = clocks.summary(wall0, wall1)
         sm_ghz = (clk["sm_mhz"] or 1965.0) / 1000.0
-        smem_peak = torch.cuda.get_device_properties(local).multi_processor_count * 128 * sm_ghz
-        p_kern = float(np.mean([a.elapsed_time(b) for a, b in p_ev]))
+        n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+        smem_peak = n_sm * 128 * sm_ghz  # GB/s
+        p_kern = float(np.mean(p_steps))  # the plain decode: its two launches and a few torch ops
+        p_achieved = bps * p_iters / (p_kern / 1000.0) / 1e9
+        dram_bytes = DECODE_DRAM_BYTES_PER_SHOT * shots
         line = {
             "metric": METRIC, "value": value, "unit": "shots/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -381,11 +423,13 @@ def main():
                        "network": {"weights": default_weights_path(WORKLOAD, P).name,
                                    "trained_tuples": meta.get("train", {}).get("tuples")},
                        "schedule": "pre_iter 80, num_sets 100, set_max_iter 60, gamma0 0.65, (-0.24,0.66), S=5",
-                       "l2": "256 MB buffer written between timed steps (flush)",
+                       "l2": "256 MB buffer written between timed steps (flush, outside the step events)",
                        "launch": dec.launch_info()},
             "logical_error_rate": l_ler,
             "plain": {"value": whole_job_shots_per_s(world, shots, p_ms), "unit": "shots/s", "ms_per_step": p_ms,
-                      "kernel_ms": p_kern, "logical_error_rate": p_ler,
+                      "logical_error_rate": p_ler,
+                      "roofline": {"bound": "smem", "achieved": p_achieved, "peak": smem_peak, "unit": "GB/s",
+                                   "frac": p_achieved / smem_peak, "shot_iterations_per_step": p_iters},
                       "note": "the same shots through RelayBPDecoder.decode (seeded legs), same run"},
             "learned_over_plain": p_ms / ms_step,
             "phase_ms": {"decode_kernel": kern, "network_and_selection": float(np.mean(net_ms)),
@@ -398,16 +442,17 @@ def main():
                                  "api": "LearnedRelayBPDecoder.decode per batch, results copied to pinned "
                                         "host memory before the next call", "steps": call_steps}},
             "gpu_launches": args.steps * 3,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm"], "traffic": DECODE_DRAM_BYTES_PER_SHOT * shots,
-                         "traffic_note": "ncu DRAM bytes of a 16,384-shot learned decode's two decode launches, "
-                                         "scaled per shot; far below the algorithmic bytes because each shot's "
-                                         "messages stay in shared memory",
-                         "kernel": "relaybp_decode_kernel (pre-iterations + relay legs of one step)",
+            "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                         "frac": achieved / smem_peak, "traffic": dram_bytes,
+                         "kernel": "relaybp decode kernel (pre-iterations + relay legs of one learned step)",
                          "kernel_ms": kern, "bytes_per_shot_iteration": bps, "shot_iterations_per_step": l_iters,
-                         "peak_source": peaks["source"],
-                         "smem": {"peak": smem_peak, "frac": achieved / smem_peak,
-                                  "note": "SMs x 128 B/clk x median SM clock; messages live in shared memory"}},
+                         "peak_source": f"computed: {n_sm} SMs x 128 B/clk x {sm_ghz:.3f} GHz (median sampled "
+                                        "SM clock); each shot's messages live in shared memory",
+                         "hbm": {"traffic_bytes": dram_bytes, "achieved": dram_bytes / (kern / 1000.0) / 1e9,
+                                 "peak": peaks["hbm"], "frac": dram_bytes / (kern / 1000.0) / 1e9 / peaks["hbm"],
+                                 "peak_source": peaks["source"],
+                                 "note": "ncu DRAM bytes of the two decode launches (16,384-shot capture, scaled "
+                                         "per shot): syndromes, saved states, outputs"}},
             "clocks": clk,
         }
         if not args.no_cpu_baseline:

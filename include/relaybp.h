@@ -104,20 +104,30 @@ RBP_API int rbp_decoder_destroy(rbp_decoder* d);
  * RelayBPDecoder.override_llr_columns (src/pelagos/decoder.py:785-834). */
 RBP_API int rbp_decoder_set_llr(rbp_decoder* d, const float* llr);
 
-/* Launch shape: `group_threads` threads decode one shot at a time (a
- * multiple of 32, at most 1024) and a thread block holds `groups_per_block`
- * such groups.  0/0 picks a default.  Fails with RBP_ERR_UNSUPPORTED when the
- * shape's shared memory does not fit. */
-RBP_API int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block);
+/* Launch shape (no reference counterpart: the reference autotunes Triton
+ * tile sizes instead, src/pelagos/autotune.py:302-541).  A group of
+ * `group_threads` threads (a multiple of 32, at most 1024) decodes
+ * `shots_per_group` shots at once (1 or 2) and a thread block holds
+ * `groups_per_block` such groups (two-shot groups: one per block).  Zeros
+ * pick the defaults.  Results do not depend on the shape.  Fails with
+ * RBP_ERR_UNSUPPORTED when the shape's registers or shared memory do not fit. */
+RBP_API int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block,
+                                  int32_t shots_per_group);
 
-/* Shared-memory bytes of one group and of the block-wide tables for the
- * current message type; the shape currently configured. */
+/* Shared-memory bytes of one shot's region and of the block-wide tables for
+ * the current message type; the shape currently configured.  Any pointer may
+ * be NULL. */
 RBP_API int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem,
-                      int32_t* group_threads, int32_t* groups_per_block, int32_t* blocks);
+                      int32_t* group_threads, int32_t* groups_per_block, int32_t* blocks,
+                      int32_t* shots_per_group);
 
 /* Per-call inputs (device memory).  Optional pointers may be NULL.
- * Mirrors decode()'s keyword arguments (src/pelagos/decoder.py:2317-2361). */
+ * Mirrors decode()'s keyword arguments (src/pelagos/decoder.py:2317-2361).
+ * struct_size must hold sizeof(rbp_batch) (RBP_BATCH_SIZE): a caller whose
+ * declaration of the struct has other fields (an older or hand-written
+ * binding) is rejected with RBP_ERR_ARGUMENT before any field is read. */
 typedef struct {
+  uint32_t struct_size;            /* sizeof(rbp_batch) */
   const uint8_t* syndromes;        /* [B, C] bits in the low bit of each byte */
   const float* llr_per_shot;       /* [B, V] prior_llr, overrides the shared LLRs */
   const float* gamma_pre;          /* [B, V] init_gamma for the first phase */
@@ -164,8 +174,10 @@ typedef struct {
   int32_t parity_first;
 } rbp_batch;
 
-/* Outputs (device memory).  Any may be NULL except found_count/iterations. */
+/* Outputs (device memory).  Any may be NULL except found_count/iterations.
+ * struct_size must hold sizeof(rbp_outputs) (RBP_OUTPUTS_SIZE), as for rbp_batch. */
 typedef struct {
+  uint32_t struct_size;            /* sizeof(rbp_outputs) */
   uint8_t* errors;                 /* [B, V] 0/1 */
   uint32_t* errors_packed;         /* [B, ceil(V/32)] bit v%32 of word v/32 */
   float* weights;                  /* [B] selected solution weight, +inf when none */
@@ -174,6 +186,9 @@ typedef struct {
   int32_t* iterations;             /* [B] BP iterations the shot ran */
   void* last_posterior;            /* [B, V] f32 (f64 for RBP_MSG_F64) posterior at the end */
 } rbp_outputs;
+
+#define RBP_BATCH_SIZE ((uint32_t)sizeof(rbp_batch))
+#define RBP_OUTPUTS_SIZE ((uint32_t)sizeof(rbp_outputs))
 
 /* Bytes of one shot's saved state (rbp_batch.resume_state / suspend_state). */
 RBP_API int rbp_state_bytes(const rbp_decoder* d, int64_t* bytes_per_shot);
@@ -258,8 +273,15 @@ RBP_API int rbp_mixed_query(const rbp_mixed* m, int32_t i, int32_t* group_thread
  * wrong results; serialise them on one stream.
  *
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and caches it.  Make that first call before any
- * stream capture begins.
+ * (cudaGetSymbolAddress) and caches it; host threads may make that first call
+ * concurrently.  Make that first call before any stream capture begins.
+ *
+ * The tables are copied from host memory that exists only during the call, so
+ * a call on a stream that is being captured returns RBP_ERR_UNSUPPORTED
+ * without enqueuing anything: a recorded copy would read freed memory when
+ * the graph is replayed.  The graph arrays are checked as rbp_graph_create
+ * checks them (RBP_ERR_ARGUMENT for a var_edges that is not the
+ * variable-major permutation of edge_var).
  */
 RBP_API int rbp_decode_static(int32_t C, int32_t V, int32_t E,
                               const int32_t* chk_ptr, const int32_t* edge_var,

@@ -83,8 +83,19 @@ class RbpParams(ct.Structure):
     ]
 
 
-class RbpBatch(ct.Structure):
+class _Sized(ct.Structure):
+    """A struct whose first field, struct_size, carries sizeof(struct): filled in on construction,
+    so the library can reject a caller whose declaration differs from include/relaybp.h."""
+
+    def __init__(self, *args, **kw):
+        super().__init__(*args, **kw)
+        if "struct_size" not in kw:
+            self.struct_size = ct.sizeof(self)
+
+
+class RbpBatch(_Sized):
     _fields_ = [
+        ("struct_size", ct.c_uint32),
         ("syndromes", ct.c_void_p),
         ("llr_per_shot", ct.c_void_p),
         ("gamma_pre", ct.c_void_p),
@@ -119,8 +130,9 @@ class RbpNetHparams(ct.Structure):
     ]
 
 
-class RbpOutputs(ct.Structure):
+class RbpOutputs(_Sized):
     _fields_ = [
+        ("struct_size", ct.c_uint32),
         ("errors", ct.c_void_p),
         ("errors_packed", ct.c_void_p),
         ("weights", ct.c_void_p),
@@ -154,9 +166,9 @@ def _declare(lib):
     lib.rbp_decoder_set_llr.restype = ct.c_int
     lib.rbp_decoder_set_llr.argtypes = [P, f32p]
     lib.rbp_decoder_configure.restype = ct.c_int
-    lib.rbp_decoder_configure.argtypes = [P, i32, i32]
+    lib.rbp_decoder_configure.argtypes = [P, i32, i32, i32]
     lib.rbp_decoder_query.restype = ct.c_int
-    lib.rbp_decoder_query.argtypes = [P, ct.POINTER(i64), ct.POINTER(i64), i32p, i32p, i32p]
+    lib.rbp_decoder_query.argtypes = [P, ct.POINTER(i64), ct.POINTER(i64), i32p, i32p, i32p, i32p]
     lib.rbp_state_bytes.restype = ct.c_int
     lib.rbp_state_bytes.argtypes = [P, ct.POINTER(i64)]
     lib.rbp_state_posterior_offset.restype = ct.c_int

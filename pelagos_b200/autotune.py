@@ -1,18 +1,27 @@
 """Launch-shape autotuner for the decode kernel.
 
-The kernel's shape is (group_threads, groups_per_block): how many threads share
-one shot (and so how many variables and checks each thread owns), and how many
-shots a thread block decodes at once.  ``tune`` times candidate shapes on a
-sample batch with CUDA events and keeps the fastest.  The choice is cached in a
-JSON file keyed by device name, graph sparsity hash, message type and the
-decode parameters, in the way the reference keys its tuning cache
-(src/pelagos/autotune.py:130-133, 222-541):
+The kernel's shape is (group_threads, groups_per_block, shots_per_group): how
+many threads share one shot (and so how many variables and checks each thread
+owns), how many groups a thread block holds, and how many shots a group
+decodes at once (1: relaybp_decode_kernel; 2: relaybp_slots_kernel, one group
+per block).  ``tune`` times candidate shapes on a sample batch with CUDA events
+(the median of ``repeats`` timed runs after a warm-up, by default of
+``decoder.decode`` and optionally of any decode call, e.g. a learned decode)
+and keeps the fastest.  The choice is cached in a JSON file keyed by device
+name, graph sparsity hash, message type and the decode parameters, in the way
+the reference keys its tuning cache (src/pelagos/autotune.py:130-133, 222-541):
 
 * cache file: ``$PELAGOS_B200_TUNE_CACHE`` or ``~/.cache/pelagos_b200_tune.json``;
 * candidates: every warp multiple G from 32 to 1024 that gives at most 16
   variables and 32 checks per thread, each with the largest group count that
-  fits (and, for one-warp groups, also half of it);
+  fits (and, for one-warp groups, also half of it), and the same G values for
+  two-shot groups;
 * a candidate the library rejects (shared memory, registers) is skipped.
+
+``default_shape`` returns the shape measured best for a workload and
+committed with the package (``data/launch_shapes.json``, keyed by graph
+sparsity hash and message type), so a fresh machine starts from a measured
+shape instead of re-tuning on a noisy sample.
 """
 
 from __future__ import annotations
@@ -21,8 +30,9 @@ import json
 import os
 import threading
 from pathlib import Path
-from typing import Iterable, List, Optional, Tuple
+from typing import Callable, Iterable, List, Optional, Tuple
 
+import numpy as np
 import torch
 
 _LOCK = threading.Lock()
@@ -62,54 +72,78 @@ def _store(key: str, value) -> None:
             pass  # a read-only home only loses the cache
 
 
-def candidates(C: int, V: int) -> List[Tuple[int, int]]:
+def candidates(C: int, V: int) -> List[Tuple[int, int, int]]:
     out = []
-    for G in range(32, 1025, 32):
-        need = -(-V // G)
-        if need > 16 or -(-C // G) > 32:
-            continue
-        out.append((G, 0))
-        if G == 32:
-            out.append((G, 8))
+    for ns in (1, 2):
+        for G in range(32, 1025, 32):
+            need = -(-V // G)
+            if need > 16 or -(-C // G) > 32:
+                continue
+            out.append((G, 0 if ns == 1 else 1, ns))
+            if G == 32 and ns == 1:
+                out.append((G, 8, 1))
     return out
 
 
-def lookup(dec, B: int) -> Optional[Tuple[int, int]]:
+def lookup(dec, B: int) -> Optional[Tuple[int, ...]]:
     v = _load().get(cache_key(dec, B))
     return tuple(v["shape"]) if v else None
 
 
-def tune(dec, syndromes: torch.Tensor, shapes: Optional[Iterable[Tuple[int, int]]] = None, repeats: int = 2,
-         use_cache: bool = True, verbose: bool = False) -> Tuple[int, int]:
-    """Time the candidate shapes on `syndromes` (device tensor); configure and return the fastest."""
+SHAPES_FILE = Path(__file__).resolve().parent / "data" / "launch_shapes.json"
+
+
+def default_shape(dec) -> Optional[Tuple[int, int, int]]:
+    """The committed shape for this graph and message type, or None."""
+    try:
+        table = json.loads(SHAPES_FILE.read_text())
+    except (OSError, ValueError):
+        return None
+    v = table.get(f"{dec.graph.sparsity_hash}|{dec.dtype_str}")
+    return tuple(v["shape"]) if v else None
+
+
+def _time(fn: Callable[[], object], repeats: int) -> float:
+    """Median of `repeats` event-timed calls after one warm-up call."""
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(repeats):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def tune(dec, syndromes: torch.Tensor, shapes: Optional[Iterable[Tuple[int, ...]]] = None, repeats: int = 5,
+         use_cache: bool = True, verbose: bool = False,
+         decode_fn: Optional[Callable[[torch.Tensor], object]] = None) -> Tuple[int, ...]:
+    """Time the candidate shapes on `syndromes` (device tensor) with ``decode_fn`` (default
+    ``dec.decode``); configure and return the fastest (median of ``repeats`` runs)."""
     B = int(syndromes.shape[0])
-    key = cache_key(dec, B)
-    if use_cache:
+    key = cache_key(dec, B) + ("" if decode_fn is None else "|custom")
+    if use_cache and decode_fn is None:
         hit = lookup(dec, B)
         if hit is not None:
             dec.configure_launch(*hit)
             return hit
+    fn = decode_fn or dec.decode
     results = []
     shapes = list(shapes) if shapes is not None else candidates(dec.C, dec.V)
-    for G, NG in shapes:
+    for shape in shapes:
         try:
-            dec.configure_launch(G, NG)
+            dec.configure_launch(*shape)
         except (NotImplementedError, ValueError):
             continue
-        dec.decode(syndromes)  # warm-up
-        torch.cuda.synchronize()
-        best = float("inf")
-        for _ in range(repeats):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            dec.decode(syndromes)
-            e1.record()
-            torch.cuda.synchronize()
-            best = min(best, e0.elapsed_time(e1))
+        ms = _time(lambda: fn(syndromes), repeats)
         info = dec.launch_info()
-        results.append((best, (info["group_threads"], info["groups_per_block"])))
+        got = (info["group_threads"], info["groups_per_block"], info["shots_per_group"])
+        results.append((ms, got))
         if verbose:
-            print(f"  G={G:4d} groups={info['groups_per_block']:2d}: {best:8.3f} ms", flush=True)
+            print(f"  G={got[0]:4d} groups={got[1]:2d} shots/group={got[2]}: {ms:8.3f} ms", flush=True)
     if not results:
         raise RuntimeError("no launch shape could be configured")
     ms, shape = min(results)

@@ -5,10 +5,12 @@
 #include "relaybp.h"
 #include "relaybp_host.h"
 #include "relaybp_kernel.cuh"
+#include "relaybp_slots.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstdint>
@@ -48,6 +50,7 @@ struct rbp_decoder {
   // launch shape
   KernelFn kernel = nullptr;
   int group_threads = 0, groups = 0, blocks = 0, vpt = 0;
+  int nshots = 1;              // shots a group decodes at once (2: relaybp_slots_kernel)
   int group_bytes = 0, block_bytes = 0;
   int sm_count = 0;
   size_t max_smem = 0;
@@ -102,7 +105,7 @@ Layout make_layout(int C, int V, int rows, int msg_type, int group_threads) {
   L.g_first = q;
   q = align16(q + 4 * W);
   L.g_red = q;
-  q = align16(q + 8 * (group_threads / 32 + 1));
+  q = align16(q + 8 * (group_threads / 32 + 4));
   L.group_bytes = q;
   return L;
 }
@@ -117,6 +120,16 @@ KernelFn pick_kernel(int msg_type, int dc, int dv, int vpt) {
   }
 }
 
+KernelFn pick_slots_kernel(int msg_type, int dc, int dv, int vpt) {
+  switch (msg_type) {
+    case RBP_MSG_F32: return rbpk::pick_slots_f32(dc, dv, vpt);
+    case RBP_MSG_F16: return rbpk::pick_slots_f16(dc, dv, vpt);
+    case RBP_MSG_BF16: return rbpk::pick_slots_bf16(dc, dv, vpt);
+    case RBP_MSG_F64: return rbpk::pick_slots_f64(dc, dv, vpt);
+    default: return nullptr;
+  }
+}
+
 // Smallest supported owned-variable count covering V with G threads.
 int vpt_for(int V, int G) {
   const int need = (V + G - 1) / G;
@@ -126,11 +139,13 @@ int vpt_for(int V, int G) {
 }
 
 // Default shape: the fewest owned variables per thread (from 3 up) whose group
-// still fits the register budget of that count, so a shot's iteration is short.
-int default_group_threads(int C, int V) {
+// still fits the register budget of that count (of the one- or two-shot
+// kernel), so a shot's iteration is short.
+int default_group_threads(int C, int V, int nshots = 1) {
   for (int vpt : {3, 4, 6, 8, 12, 16}) {
     const int G = std::max(32, (V + vpt - 1) / vpt + 31) / 32 * 32;
-    if (G <= rbpk::max_block_threads(vpt) && (C + G - 1) / G <= 32 && vpt_for(V, G) <= vpt) return G;
+    const int max_threads = nshots == 2 ? rbpk::max_slots_block_threads(vpt) : rbpk::max_block_threads(vpt);
+    if (G <= max_threads && (C + G - 1) / G <= 32 && vpt_for(V, G) <= vpt) return G;
   }
   return 256;  // configure reports why no shape fits
 }
@@ -151,17 +166,47 @@ cudaError_t set_max_dynamic_smem(const void* kernel, size_t max_smem, size_t* st
 struct Launch {
   KernelFn kernel;
   int group_threads, groups, blocks;
+  int nshots;  // 1: relaybp_decode_kernel; 2: relaybp_slots_kernel (one group per block)
 };
 
-// Kernel and launch shape for G threads per group (groups_per_block 0: as many as fit).
+// Two-shot shape: one group of G threads per block, two shot regions.
+int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int groups_per_block,
+                        size_t max_smem, int sm_count, Launch* out, const std::string& w) {
+  const int vpt = vpt_for(V, G);
+  const int max_threads = rbpk::max_slots_block_threads(vpt);
+  if (G > max_threads)
+    return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +
+                                         " variables each exceed the two-shot kernel's register budget");
+  if (groups_per_block > 1)
+    return fail(RBP_ERR_UNSUPPORTED, w + ": the two-shot kernel runs one group per block");
+  KernelFn k = pick_slots_kernel(msg_type, slots, vslots, vpt);
+  if (!k) return fail(RBP_ERR_UNSUPPORTED, w + ": no two-shot kernel for this degree / shape");
+  const Layout L = make_layout(C, V, rows, msg_type, G);
+  const size_t smem = (size_t)L.off_group0 + 2 * (size_t)L.group_bytes;
+  if (smem > max_smem)
+    return fail(RBP_ERR_UNSUPPORTED, w + ": two shots' state (" + std::to_string(2 * L.group_bytes) +
+                                         " B) does not fit in shared memory");
+  RBP_CUDA(set_max_dynamic_smem(reinterpret_cast<const void*>(k), max_smem));
+  int per_sm = 0;
+  RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G, smem));
+  if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
+  *out = Launch{k, G, 1, per_sm * sm_count, 2};
+  return RBP_OK;
+}
+
+// Kernel and launch shape for G threads per group (groups_per_block 0: as many
+// as fit) decoding `nshots` shots at once (1 or 2).
 int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int groups_per_block,
-                  size_t max_smem, int sm_count, Launch* out, const char* who) {
+                  size_t max_smem, int sm_count, Launch* out, const char* who, int nshots = 1) {
   const std::string w(who);
   if (G % 32 != 0 || G > 1024)
     return fail(RBP_ERR_ARGUMENT, w + ": group_threads must be a multiple of 32, at most 1024");
+  if (nshots != 1 && nshots != 2) return fail(RBP_ERR_ARGUMENT, w + ": shots_per_group must be 1 or 2");
   const int vpt = vpt_for(V, G);
   if (vpt < 0) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 16 variables per thread; use more group threads");
   if ((C + G - 1) / G > 32) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 32 checks per thread; use more group threads");
+  if (nshots == 2)
+    return choose_slots_launch(C, V, slots, vslots, rows, msg_type, G, groups_per_block, max_smem, sm_count, out, w);
   const int max_threads = rbpk::max_block_threads(vpt);
   if (G > max_threads)
     return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +
@@ -185,13 +230,21 @@ int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, i
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * NG, smem));
   if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
-  *out = Launch{k, G, NG, per_sm * sm_count};
+  *out = Launch{k, G, NG, per_sm * sm_count, 1};
   return RBP_OK;
 }
 
 int check_batch(const char* who, int64_t B, const rbp_batch* in, const rbp_outputs* out, const rbp_params& p,
                 int n_alpha) {
   const std::string w(who);
+  if (in->struct_size != sizeof(rbp_batch))
+    return fail(RBP_ERR_ARGUMENT, w + ": rbp_batch.struct_size is " + std::to_string(in->struct_size) +
+                                      ", this library's rbp_batch has " + std::to_string(sizeof(rbp_batch)) +
+                                      " bytes (the caller's declaration differs from include/relaybp.h)");
+  if (out->struct_size != sizeof(rbp_outputs))
+    return fail(RBP_ERR_ARGUMENT, w + ": rbp_outputs.struct_size is " + std::to_string(out->struct_size) +
+                                      ", this library's rbp_outputs has " + std::to_string(sizeof(rbp_outputs)) +
+                                      " bytes (the caller's declaration differs from include/relaybp.h)");
   if (B < 0) return fail(RBP_ERR_ARGUMENT, w + ": negative batch");
   if (B > INT_MAX) return fail(RBP_ERR_UNSUPPORTED, w + ": batch exceeds 2^31-1 shots");
   if (B == 0) return RBP_OK;
@@ -272,9 +325,10 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.g_best = L.g_best;
   a.g_first = L.g_first;
   a.g_red = L.g_red;
-  const long long need_blocks = (B + lc.groups - 1) / lc.groups;
+  const long long per_block = (long long)lc.groups * lc.nshots;  // shots a block decodes at once
+  const long long need_blocks = (B + per_block - 1) / per_block;
   const int blocks = (int)std::min<long long>(lc.blocks, need_blocks);
-  const size_t smem = (size_t)L.off_group0 + (size_t)lc.groups * L.group_bytes;
+  const size_t smem = (size_t)L.off_group0 + (size_t)per_block * L.group_bytes;
   cudaError_t e = cudaMemsetAsync(queue, 0, sizeof(int), st);
   if (e != cudaSuccess) return fail(RBP_ERR_CUDA, std::string(who) + ": cudaMemsetAsync: " + cudaGetErrorString(e));
   lc.kernel<<<blocks, lc.group_threads * lc.groups, smem, st>>>(dgph, a);
@@ -288,18 +342,20 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
 static __device__ __align__(256) unsigned char g_static_scratch[RBP_STATIC_SCRATCH_BYTES];
 
 // Device address of g_static_scratch on `device` (the current device), looked
-// up on the first call per device and cached.
+// up on the first call per device and cached.  Host threads may race on a
+// device's first lookup: both store the same address, and the atomics make
+// that race well defined.
 int static_scratch(int device, unsigned char** out) {
-  static void* cached[64] = {};
+  static std::atomic<void*> cached[64];
   if (device < 0 || device >= 64) return fail(RBP_ERR_UNSUPPORTED, "rbp_decode_static: device ordinal above 63");
-  if (!cached[device]) {
-    void* ptr = nullptr;
+  void* ptr = cached[device].load(std::memory_order_relaxed);
+  if (!ptr) {
     const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
     if (e != cudaSuccess)
       return fail(RBP_ERR_CUDA, std::string("rbp_decode_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    cached[device] = ptr;
+    cached[device].store(ptr, std::memory_order_relaxed);
   }
-  *out = static_cast<unsigned char*>(cached[device]);
+  *out = static_cast<unsigned char*>(ptr);
   return RBP_OK;
 }
 
@@ -383,14 +439,16 @@ int rbp_graph_destroy(rbp_graph* g) {
   return RBP_OK;
 }
 
-int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block) {
+int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block,
+                          int32_t shots_per_group) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: null decoder");
   const rbp_graph* g = d->g;
-  const int G = group_threads > 0 ? group_threads : default_group_threads(g->C, g->V);
+  const int nshots = shots_per_group > 0 ? shots_per_group : 1;
+  const int G = group_threads > 0 ? group_threads : default_group_threads(g->C, g->V, nshots);
   DeviceGuard dg(g->device);
   Launch lc{};
   const int rc = choose_launch(g->C, g->V, g->slots, g->vslots, d->rows, d->p.msg_type, G, groups_per_block,
-                               d->max_smem, d->sm_count, &lc, "rbp_decoder_configure");
+                               d->max_smem, d->sm_count, &lc, "rbp_decoder_configure", nshots);
   if (rc != RBP_OK) return rc;
   const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, G);
   d->kernel = lc.kernel;
@@ -398,6 +456,7 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
   d->group_threads = lc.group_threads;
   d->groups = lc.groups;
   d->blocks = lc.blocks;
+  d->nshots = lc.nshots;
   d->group_bytes = L.group_bytes;
   d->block_bytes = L.off_group0;
   return RBP_OK;
@@ -455,7 +514,7 @@ int rbp_decoder_create(const rbp_graph* g, const rbp_params* p, const float* llr
   int zero = 0, rc;
   if ((rc = d->gamma_legs.upload(gamma_legs, (size_t)p->num_sets * g->V)) ||
       (rc = d->alpha.upload(a_host.data(), a_host.size())) || (rc = d->queue.upload(&zero, 1)) ||
-      (rc = rbp_decoder_set_llr(d, llr)) || (rc = rbp_decoder_configure(d, 0, 0))) {
+      (rc = rbp_decoder_set_llr(d, llr)) || (rc = rbp_decoder_configure(d, 0, 0, 0))) {
     delete d;
     return rc;
   }
@@ -490,8 +549,9 @@ int rbp_state_posterior_offset(const rbp_decoder* d, int64_t* offset) {
 }
 
 int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem, int32_t* group_threads,
-                      int32_t* groups_per_block, int32_t* blocks) {
+                      int32_t* groups_per_block, int32_t* blocks, int32_t* shots_per_group) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_query: null decoder");
+  if (shots_per_group) *shots_per_group = d->nshots;
   if (group_smem) *group_smem = d->group_bytes;
   if (block_smem) *block_smem = d->block_bytes;
   if (group_threads) *group_threads = d->group_threads;
@@ -509,7 +569,7 @@ int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs
   if (!dg.ok) return fail(RBP_ERR_CUDA, "rbp_decode: cannot select the CUDA device");
   const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, d->group_threads);
   const DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
-  const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks};
+  const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks, d->nshots};
   return launch_decode(dgph, d->p, L, lc, d->llr.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
                        out, reinterpret_cast<cudaStream_t>(stream), "rbp_decode");
 }
@@ -837,12 +897,35 @@ int rbp_decode_static(int32_t C, int32_t V, int32_t E, const int32_t* chk_ptr, c
                                          std::to_string((long long)RBP_STATIC_SCRATCH_BYTES));
   const int rc0 = check_batch(who, B, in, out, *p, p->use_alpha ? n_alpha : 1);
   if (rc0 != RBP_OK || B == 0) return rc0;
+  // var_edges must list every edge once, under its own variable (rbp_graph_create's
+  // test).  E <= rows * C < 65535, so a fixed 8 KiB bitmap holds the edges seen.
+  {
+    uint32_t seen[65536 / 32] = {};
+    for (int v = 0; v < V; ++v)
+      for (int q = var_ptr[v]; q < var_ptr[v + 1]; ++q) {
+        const int e = var_edges[q];
+        if (e < 0 || e >= E || edge_var[e] != v || (seen[e >> 5] >> (e & 31)) & 1u)
+          return fail(RBP_ERR_ARGUMENT,
+                      std::string(who) + ": var_edges is not the variable-major permutation of edge_var");
+        seen[e >> 5] |= 1u << (e & 31);
+      }
+  }
   DeviceGuard dg(device);
   if (!dg.ok) return fail(RBP_ERR_CUDA, std::string(who) + ": cannot select the CUDA device");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // The tables are copied from host memory that exists only during this call,
+  // so a copy recorded into a graph would read freed memory when replayed.
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    RBP_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(RBP_ERR_UNSUPPORTED, std::string(who) +
+                                           ": the stream is being captured; this call copies its tables from host "
+                                           "memory that is gone when a graph replays, so it runs on eager streams only");
+  }
   unsigned char* scratch = nullptr;
   int rc = static_scratch(device, &scratch);
   if (rc != RBP_OK) return rc;
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 
   // Tables are staged through a fixed stack buffer; a pageable-memory copy has
   // consumed the buffer when cudaMemcpyAsync returns, so the buffer is reused.
@@ -866,9 +949,7 @@ int rbp_decode_static(int32_t C, int32_t V, int32_t E, const int32_t* chk_ptr, c
       uint16_t pos = rbpk::kNoSlot;
       const int q = var_ptr[v] + k;
       if (q < var_ptr[v + 1]) {
-        const int e = var_edges[q];
-        if (e < 0 || e >= E || edge_var[e] != v)
-          return fail(RBP_ERR_ARGUMENT, std::string(who) + ": var_edges is not the variable-major order of edge_var");
+        const int e = var_edges[q];  // validated above
         const int c = (int)(std::upper_bound(chk_ptr, chk_ptr + C + 1, e) - chk_ptr) - 1;  // check of edge e
         pos = (uint16_t)slot_index_host(e - chk_ptr[c], c, C, p->msg_type);
       }

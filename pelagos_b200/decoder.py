@@ -98,17 +98,17 @@ class _NativeDecoder:
         llr = np.ascontiguousarray(llr, dtype=np.float32)
         nat.check(nat.lib().rbp_decoder_set_llr(self._dec, nat.f32_ptr(llr)), "rbp_decoder_set_llr")
 
-    def configure(self, group_threads: int, groups_per_block: int):
-        nat.check(nat.lib().rbp_decoder_configure(self._dec, int(group_threads), int(groups_per_block)),
-                  "rbp_decoder_configure")
+    def configure(self, group_threads: int, groups_per_block: int, shots_per_group: int = 0):
+        nat.check(nat.lib().rbp_decoder_configure(self._dec, int(group_threads), int(groups_per_block),
+                                                  int(shots_per_group)), "rbp_decoder_configure")
 
     def query(self) -> dict:
         gs, bs = ct.c_int64(), ct.c_int64()
-        gt, gb, nb = ct.c_int32(), ct.c_int32(), ct.c_int32()
+        gt, gb, nb, ns = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_int32()
         nat.check(nat.lib().rbp_decoder_query(self._dec, ct.byref(gs), ct.byref(bs), ct.byref(gt),
-                                              ct.byref(gb), ct.byref(nb)), "rbp_decoder_query")
+                                              ct.byref(gb), ct.byref(nb), ct.byref(ns)), "rbp_decoder_query")
         return {"group_smem": gs.value, "block_smem": bs.value, "group_threads": gt.value,
-                "groups_per_block": gb.value, "blocks": nb.value}
+                "groups_per_block": gb.value, "blocks": nb.value, "shots_per_group": ns.value}
 
     def decode(self, B: int, batch: nat.RbpBatch, outs: nat.RbpOutputs, stream: int):
         nat.check(nat.lib().rbp_decode(self._dec, int(B), ct.byref(batch), ct.byref(outs),
@@ -137,7 +137,8 @@ class RelayBPDecoder:
 
     * ``mix_rounding``: rounding of the memory mix (1-g)*llr + g*posterior:
       "separate" (default; one rounding per operation), "fma_gp" or "fma_lp";
-    * ``launch``: optional (group_threads, groups_per_block) kernel shape.
+    * ``launch``: optional (group_threads, groups_per_block[, shots_per_group]) kernel shape;
+      shots_per_group 2 selects the kernel whose groups decode two shots at once.
     * ``hard_shots_first`` (default True): a relay decode of at least 1024 shots
       runs as two launches, the pre-iterations and then the relay legs resumed
       from each shot's saved state, with the shots the pre-iterations left
@@ -377,9 +378,10 @@ class RelayBPDecoder:
 
     # ------------------------------------------------------------------ public helpers
 
-    def configure_launch(self, group_threads: int, groups_per_block: int) -> None:
-        """Set the kernel shape (threads per shot group, groups per thread block)."""
-        self._launch = (int(group_threads), int(groups_per_block))
+    def configure_launch(self, group_threads: int, groups_per_block: int, shots_per_group: int = 0) -> None:
+        """Set the kernel shape (threads per shot group, groups per thread block, shots a group
+        decodes at once; 0 picks the default)."""
+        self._launch = (int(group_threads), int(groups_per_block), int(shots_per_group))
         for nd in self._native.values():
             nd.configure(*self._launch)
 

@@ -22,10 +22,13 @@ priors, the syndromes, every constructor / decode argument, the gamma rows the
 legs used, the reference's variable-edge order (``var_edges``, built with a
 non-stable ``np.argsort`` in src/pelagos/graph.py:145) and the decode outputs.
 
-This script reads the reference from ``/root/reference/src`` and so only runs
-where that tree exists; the fixtures it writes are what the tests consume.
+This script imports the reference from the directory named by the environment
+variable ``PELAGOS_REF_SRC`` (the ``src`` directory of a pelagos checkout) and so
+only runs where such a tree exists; the fixtures it writes are what the tests
+consume.
 
-Usage: ``python tests/golden/make_golden.py [case ...]`` (default: all cases).
+Usage: ``PELAGOS_REF_SRC=<pelagos>/src python tests/golden/make_golden.py [case ...]``
+(default: all cases).
 """
 
 from __future__ import annotations
@@ -37,7 +40,9 @@ import time
 from pathlib import Path
 
 os.environ["TRITON_INTERPRET"] = "1"
-REF_SRC = "/root/reference/src"
+REF_SRC = os.environ.get("PELAGOS_REF_SRC")
+if not REF_SRC or not Path(REF_SRC, "pelagos", "decoder.py").exists():
+    raise SystemExit("set PELAGOS_REF_SRC to the src directory of a pelagos checkout")
 sys.path.insert(0, REF_SRC)
 
 import numpy as np  # noqa: E402
@@ -263,6 +268,24 @@ def _cases():
                   algo="relay", data_type="float32", seed=7)
         return H, pr, S, kw, dict(skip_relay_legs=True, return_last_posterior=True)
     cases["regular300x600_pre3"] = regular_pre3
+
+    # The full Relay-BP-S schedule of every benchmark configuration (pre 80, 100 legs of at most
+    # 60 iterations, gamma0 0.65, U(-0.24, 0.66) legs, stop_nconv 5: decoder.py:271-307 defaults).
+    full = dict(pre_iter=80, num_sets=100, set_max_iter=60, gamma0=0.65, gamma_dist_interval=(-0.24, 0.66),
+                stop_nconv=5, algo="relay", data_type="float32", seed=1234)
+    cases["bb72_full_schedule"] = lambda: (*_bb72_case(6, seed=31), dict(full), {})
+    cases["bb72_full_schedule_plain"] = lambda: (*_bb72_case(4, seed=32), dict(full, algo="plain"), {})
+
+    def bb144_phen(B, p, seed):
+        w = codes.workload("bb144_phen", p=p)
+        err, syn = w.sample(B, seed=seed)
+        return w.H, w.priors, syn
+
+    # the benchmark's [[144,12,12]] phenomenological matrix (936 x 2592) with a short schedule
+    cases["bb144_phen_short"] = lambda: (
+        *bb144_phen(2, 0.004, 41),
+        dict(pre_iter=6, num_sets=2, set_max_iter=4, gamma0=0.65, gamma_dist_interval=(-0.24, 0.66),
+             stop_nconv=2, algo="relay", data_type="float32", seed=1234), {})
     return cases
 
 

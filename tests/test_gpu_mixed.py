@@ -70,7 +70,7 @@ def test_autotune_keeps_results(tmp_path, monkeypatch):
     syn = torch.from_numpy(w.sample(2048, seed=17)[1]).to(DEV)
     dec = RelayBPDecoder(w.H, w.priors, **RELAY)
     ref = _np(dec.decode(syn))
-    shape = autotune.tune(dec, syn, shapes=[(256, 0), (512, 0), (864, 0)], repeats=1)
+    shape = autotune.tune(dec, syn, shapes=[(256, 0), (512, 0), (864, 0), (448, 1, 2)], repeats=1)
     assert dec.launch_info()["group_threads"] == shape[0]
     got = _np(dec.decode(syn))
     for k in KEYS:

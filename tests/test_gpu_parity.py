@@ -52,8 +52,13 @@ def _golden_decode_kwargs(g):
     return d
 
 
-def test_reference_fixtures_bit_exact(golden):
-    dec = _golden_decoder(golden)
+#: shots a group decodes at once: the one-shot kernel and the two-shot kernel
+NSHOTS = [1, 2]
+
+
+@pytest.mark.parametrize("nshots", NSHOTS)
+def test_reference_fixtures_bit_exact(golden, nshots):
+    dec = _golden_decoder(golden, launch=(0, 0, nshots))
     out = _np(dec.decode(torch.from_numpy(golden.syndromes).to(DEV), **_golden_decode_kwargs(golden)))
     z = golden.z
     np.testing.assert_array_equal(out["errors"], z["out_errors"])
@@ -86,22 +91,24 @@ def _assert_same(out, ref, keys=KEYS):
             raise AssertionError(f"{k} differs on {len(bad)} shots, first {bad[:8].tolist()}")
 
 
+@pytest.mark.parametrize("nshots", NSHOTS)
 @pytest.mark.parametrize("dtype", ["float32", "float16", "bfloat16", "float64"])
-def test_bb72_code_capacity_matches_oracle(dtype):
+def test_bb72_code_capacity_matches_oracle(dtype, nshots):
     w = codes.workload("bb72_cc")
     err, syn = w.sample(1024 if dtype == "float32" else 256, seed=7)
-    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, launch=(0, 0, nshots), **RELAY)
     out = _np(dec.decode(torch.from_numpy(syn).to(DEV), return_last_posterior=True))
     ref = _oracle_for(dec, syn)
     _assert_same(out, ref)
     np.testing.assert_array_equal(out["last_posterior"].astype(np.float64), ref["last_posterior"])
 
 
+@pytest.mark.parametrize("nshots", NSHOTS)
 @pytest.mark.parametrize("dtype", ["float32", "float16", "bfloat16"])
-def test_bb144_phenomenological_matches_oracle(dtype):
+def test_bb144_phenomenological_matches_oracle(dtype, nshots):
     w = codes.workload("bb144_phen")
     err, syn = w.sample(384, seed=11)
-    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, launch=(0, 0, nshots), **RELAY)
     out = _np(dec.decode(torch.from_numpy(syn).to(DEV)))
     _assert_same(out, _oracle_for(dec, syn))
 
@@ -112,7 +119,8 @@ def test_bb144_phenomenological_matches_oracle(dtype):
     dict(unconverged_correction="last_leg"), dict(set_max_iter=0), dict(pre_iter=3, num_sets=5, set_max_iter=4),
     dict(mix_rounding="fma_gp"), dict(mix_rounding="fma_lp"),
 ])
-def test_options_match_oracle(variant):
+@pytest.mark.parametrize("nshots", NSHOTS)
+def test_options_match_oracle(variant, nshots):
     w = codes.workload("bb72_cc", p=0.08)
     err, syn = w.sample(512, seed=3)
     variant = dict(variant)
@@ -120,12 +128,13 @@ def test_options_match_oracle(variant):
     kw.update(pre_iter=20, num_sets=12, set_max_iter=15)
     mix = variant.pop("mix_rounding", "separate")
     kw.update(variant)
-    dec = RelayBPDecoder(w.H, w.priors, mix_rounding=mix, **kw)
+    dec = RelayBPDecoder(w.H, w.priors, mix_rounding=mix, launch=(0, 0, nshots), **kw)
     out = _np(dec.decode(torch.from_numpy(syn).to(DEV)))
     _assert_same(out, _oracle_for(dec, syn, mix=mix))
 
 
-def test_per_shot_inputs_match_oracle():
+@pytest.mark.parametrize("nshots", NSHOTS)
+def test_per_shot_inputs_match_oracle(nshots):
     w = codes.workload("bb144_cc")
     err, syn = w.sample(256, seed=5)
     rng = np.random.default_rng(9)
@@ -135,7 +144,7 @@ def test_per_shot_inputs_match_oracle():
     pl = rng.uniform(2.5, 4.5, (256, V)).astype(np.float32)
     lg = rng.uniform(-0.24, 0.66, (256, 3, V)).astype(np.float32)
     kw = dict(RELAY, pre_iter=25, num_sets=8, set_max_iter=20, stop_nconv=3)
-    dec = RelayBPDecoder(w.H, w.priors, **kw)
+    dec = RelayBPDecoder(w.H, w.priors, launch=(0, 0, nshots), **kw)
     t = lambda a: torch.from_numpy(a).to(DEV)  # noqa: E731
     out = _np(dec.decode(t(syn), init_posterior=t(ip), init_gamma=t(ig), prior_llr=t(pl), leg_gammas=t(lg),
                          pre_iter_override=30, return_last_posterior=True))
@@ -231,7 +240,8 @@ def test_full_size_batch_and_permutation_invariance(bb144_full):
         np.testing.assert_array_equal(sub[k], out[k][idx])
 
 
-@pytest.mark.parametrize("shape", [(192, 1), (256, 1), (448, 1), (512, 1), (768, 1), (864, 1)])
+@pytest.mark.parametrize("shape", [(192, 1), (256, 1), (448, 1), (512, 1), (768, 1), (864, 1),
+                                   (256, 1, 2), (384, 1, 2), (448, 1, 2), (480, 1, 2)])
 def test_launch_shape_invariance(shape):
     w = codes.workload("bb144_phen")
     err, syn = w.sample(512, seed=12)

@@ -37,17 +37,24 @@ def _ptr(t):
 
 
 def _static_decode(dec: RelayBPDecoder, syn: torch.Tensor) -> dict:
-    """One rbp_decode_static call with the decoder's graph, priors and leg table."""
+    """One rbp_decode_static call with the decoder's graph, priors, leg table and (for
+    normalized min-sum) its per-iteration alpha table, all in device memory."""
+    from pelagos_b200.utils import alpha_schedule
+
     g = dec.graph
     B = int(syn.shape[0])
     llr = torch.from_numpy(dec.log_prior_ratios).to(DEV)
     legs = torch.from_numpy(np.ascontiguousarray(dec._leg_table(0))).to(DEV)
+    use_alpha, alpha = alpha_schedule(dec.normalized_min_sum_alpha, dec.alpha_iteration_scaling_factor,
+                                      max(dec.pre_iter, dec.set_max_iter, 1))
+    alpha_dev = torch.from_numpy(np.ascontiguousarray(alpha, np.float32)).to(DEV) if use_alpha else None
+    post_dtype = torch.float64 if dec.dtype_str == "float64" else torch.float32
     out = {
         "errors": torch.full((B, dec.V), 7, dtype=torch.uint8, device=DEV),
         "weight_fixed": torch.zeros(B, dtype=torch.int64, device=DEV),
         "found_count": torch.full((B,), -1, dtype=torch.int32, device=DEV),
         "iterations": torch.full((B,), -1, dtype=torch.int32, device=DEV),
-        "last_posterior": torch.full((B, dec.V), float("nan"), dtype=torch.float32, device=DEV),
+        "last_posterior": torch.full((B, dec.V), float("nan"), dtype=post_dtype, device=DEV),
     }
     batch = nat.RbpBatch(syndromes=_ptr(syn), llr_per_shot=None, gamma_pre=None,
                          gamma0=float(np.float32(dec.gamma0)), init_posterior=None, gamma_legs_shot=None,
@@ -58,7 +65,8 @@ def _static_decode(dec: RelayBPDecoder, syn: torch.Tensor) -> dict:
     params = dec._params()
     rc = nat.lib().rbp_decode_static(
         g.C, g.V, g.E, nat.i32_ptr(g.chk_ptr), nat.i32_ptr(g.edge_var), nat.i32_ptr(g.var_ptr),
-        nat.i32_ptr(g.var_edges), ct.byref(params), _ptr(llr), _ptr(legs), None, 0, 0, B,
+        nat.i32_ptr(g.var_edges), ct.byref(params), _ptr(llr), _ptr(legs), _ptr(alpha_dev),
+        int(alpha_dev.numel()) if alpha_dev is not None else 0, 0, B,
         ct.byref(batch), ct.byref(outs), ct.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == nat.RBP_OK, nat.lib().rbp_last_error().decode()
     torch.cuda.synchronize()
@@ -77,12 +85,21 @@ def _assert_identical(got: dict, want: dict) -> None:
         np.testing.assert_array_equal(got[k], want[k], err_msg=k)
 
 
-@pytest.mark.parametrize("workload,shots", [("bb144_phen", 2048), ("bb72_cc", 1024)])
-def test_static_entry_matches_decoder_entry_on_two_calls(workload, shots):
+@pytest.mark.parametrize("workload,shots,extra", [
+    ("bb144_phen", 2048, {}),
+    ("bb72_cc", 1024, {}),
+    ("bb144_phen", 512, {"data_type": "float16"}),
+    ("bb144_phen", 512, {"data_type": "bfloat16"}),
+    ("bb72_cc", 512, {"data_type": "float64"}),
+    ("bb72_cc", 512, {"normalized_min_sum_alpha": 0.0}),   # alpha ramp: the alpha table is read per iteration
+    ("bb72_cc", 512, {"normalized_min_sum_alpha": 0.8, "data_type": "float16"}),
+])
+def test_static_entry_matches_decoder_entry_on_two_calls(workload, shots, extra):
+    """Every message type's slot layout and the caller-supplied alpha table, against rbp_decode."""
     w = codes.workload(workload)
     err, syn = w.sample(shots, seed=99)
     syn = torch.from_numpy(syn).to(DEV)
-    dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, **{**RELAY, **extra})
     want = _decoder_entry(dec, syn)
     first = _static_decode(dec, syn)
     second = _static_decode(dec, syn)   # the array keeps the first call's contents
@@ -123,3 +140,35 @@ def test_static_entry_rejects_tables_beyond_the_array():
     assert rc == nat.RBP_ERR_UNSUPPORTED
     msg = nat.lib().rbp_last_error().decode()
     assert "scratch" in msg and str(nat.STATIC_SCRATCH_BYTES) in msg
+
+
+def test_static_entry_refuses_a_capturing_stream():
+    """The tables are staged from host memory that is gone by the time a graph replays, so a
+    call on a stream under capture is refused before anything is enqueued."""
+    w = codes.workload("bb72_cc")
+    syn = torch.from_numpy(w.sample(64, seed=3)[1]).to(DEV)
+    dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    _static_decode(dec, syn)  # first call on the device: looks up the array's address
+    g = dec.graph
+    found = torch.zeros(64, dtype=torch.int32, device=DEV)
+    iters = torch.zeros(64, dtype=torch.int32, device=DEV)
+    llr = torch.from_numpy(dec.log_prior_ratios).to(DEV)
+    legs = torch.from_numpy(np.ascontiguousarray(dec._leg_table(0))).to(DEV)
+    batch = nat.RbpBatch(syndromes=_ptr(syn), gamma0=float(np.float32(dec.gamma0)), pre_iter=dec.pre_iter)
+    outs = nat.RbpOutputs(found_count=_ptr(found), iterations=_ptr(iters))
+    params = dec._params()
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        graph.capture_begin()
+        rc = nat.lib().rbp_decode_static(
+            g.C, g.V, g.E, nat.i32_ptr(g.chk_ptr), nat.i32_ptr(g.edge_var), nat.i32_ptr(g.var_ptr),
+            nat.i32_ptr(g.var_edges), ct.byref(params), _ptr(llr), _ptr(legs), None, 0, 0, 64,
+            ct.byref(batch), ct.byref(outs), ct.c_void_p(side.cuda_stream))
+        found.add_(1)  # something for the graph to hold
+        graph.capture_end()
+    assert rc == nat.RBP_ERR_UNSUPPORTED
+    assert "captured" in nat.lib().rbp_last_error().decode()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert int(found.sum()) == 64  # the capture itself was left intact: one recorded add
