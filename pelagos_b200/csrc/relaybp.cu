@@ -120,12 +120,12 @@ KernelFn pick_kernel(int msg_type, int dc, int dv, int vpt) {
   }
 }
 
-KernelFn pick_slots_kernel(int msg_type, int dc, int dv, int vpt) {
+KernelFn pick_slots_kernel(int msg_type, int dc, int dv, int vpt, int ns) {
   switch (msg_type) {
-    case RBP_MSG_F32: return rbpk::pick_slots_f32(dc, dv, vpt);
-    case RBP_MSG_F16: return rbpk::pick_slots_f16(dc, dv, vpt);
-    case RBP_MSG_BF16: return rbpk::pick_slots_bf16(dc, dv, vpt);
-    case RBP_MSG_F64: return rbpk::pick_slots_f64(dc, dv, vpt);
+    case RBP_MSG_F32: return rbpk::pick_slots_f32(dc, dv, vpt, ns);
+    case RBP_MSG_F16: return rbpk::pick_slots_f16(dc, dv, vpt, ns);
+    case RBP_MSG_BF16: return rbpk::pick_slots_bf16(dc, dv, vpt, ns);
+    case RBP_MSG_F64: return rbpk::pick_slots_f64(dc, dv, vpt, ns);
     default: return nullptr;
   }
 }
@@ -144,7 +144,7 @@ int vpt_for(int V, int G) {
 int default_group_threads(int C, int V, int nshots = 1) {
   for (int vpt : {3, 4, 6, 8, 12, 16}) {
     const int G = std::max(32, (V + vpt - 1) / vpt + 31) / 32 * 32;
-    const int max_threads = nshots == 2 ? rbpk::max_slots_block_threads(vpt) : rbpk::max_block_threads(vpt);
+    const int max_threads = rbpk::max_slots_block_threads(vpt, nshots);
     if (G <= max_threads && (C + G - 1) / G <= 32 && vpt_for(V, G) <= vpt) return G;
   }
   return 256;  // configure reports why no shape fits
@@ -166,31 +166,33 @@ cudaError_t set_max_dynamic_smem(const void* kernel, size_t max_smem, size_t* st
 struct Launch {
   KernelFn kernel;
   int group_threads, groups, blocks;
-  int nshots;  // 1: relaybp_decode_kernel; 2: relaybp_slots_kernel (one group per block)
+  int nshots;  // shots a group decodes at once (relaybp_slots_kernel when groups == 1)
 };
 
-// Two-shot shape: one group of G threads per block, two shot regions.
-int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int groups_per_block,
+// Block-per-group shape: one group of G threads per block with nshots shot regions
+// (relaybp_slots_kernel).
+int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int nshots,
                         size_t max_smem, int sm_count, Launch* out, const std::string& w) {
   const int vpt = vpt_for(V, G);
-  const int max_threads = rbpk::max_slots_block_threads(vpt);
+  const int max_threads = rbpk::max_slots_block_threads(vpt, nshots);
   if (G > max_threads)
     return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +
-                                         " variables each exceed the two-shot kernel's register budget");
-  if (groups_per_block > 1)
-    return fail(RBP_ERR_UNSUPPORTED, w + ": the two-shot kernel runs one group per block");
-  KernelFn k = pick_slots_kernel(msg_type, slots, vslots, vpt);
-  if (!k) return fail(RBP_ERR_UNSUPPORTED, w + ": no two-shot kernel for this degree / shape");
+                                         " variables each exceed the register budget of " + std::to_string(nshots) +
+                                         "-shot groups");
+  KernelFn k = pick_slots_kernel(msg_type, slots, vslots, vpt, nshots);
+  if (!k)
+    return fail(RBP_ERR_UNSUPPORTED, w + ": no block-per-group kernel for this degree / shape (check degrees "
+                                         "above 16 run with several groups per block, one shot each)");
   const Layout L = make_layout(C, V, rows, msg_type, G);
-  const size_t smem = (size_t)L.off_group0 + 2 * (size_t)L.group_bytes;
+  const size_t smem = (size_t)L.off_group0 + (size_t)nshots * L.group_bytes;
   if (smem > max_smem)
-    return fail(RBP_ERR_UNSUPPORTED, w + ": two shots' state (" + std::to_string(2 * L.group_bytes) +
-                                         " B) does not fit in shared memory");
+    return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(nshots) + " shots' state (" +
+                                         std::to_string(nshots * L.group_bytes) + " B) does not fit in shared memory");
   RBP_CUDA(set_max_dynamic_smem(reinterpret_cast<const void*>(k), max_smem));
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G, smem));
   if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
-  *out = Launch{k, G, 1, per_sm * sm_count, 2};
+  *out = Launch{k, G, 1, per_sm * sm_count, nshots};
   return RBP_OK;
 }
 
@@ -205,8 +207,12 @@ int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, i
   const int vpt = vpt_for(V, G);
   if (vpt < 0) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 16 variables per thread; use more group threads");
   if ((C + G - 1) / G > 32) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 32 checks per thread; use more group threads");
-  if (nshots == 2)
-    return choose_slots_launch(C, V, slots, vslots, rows, msg_type, G, groups_per_block, max_smem, sm_count, out, w);
+  // groups_per_block 1, or two shots per group: the block-per-group kernel
+  if (nshots == 2 || groups_per_block == 1) {
+    if (groups_per_block > 1)
+      return fail(RBP_ERR_UNSUPPORTED, w + ": two-shot groups run one group per block");
+    return choose_slots_launch(C, V, slots, vslots, rows, msg_type, G, nshots, max_smem, sm_count, out, w);
+  }
   const int max_threads = rbpk::max_block_threads(vpt);
   if (G > max_threads)
     return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +

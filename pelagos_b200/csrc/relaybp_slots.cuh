@@ -1,5 +1,5 @@
-// The two-shot decode kernel (sm_100a): one thread block is one group of G
-// threads that decodes NS shots at once, each in its own "slot".
+// The block-per-group decode kernel (sm_100a): one thread block is one group of
+// G threads that decodes NS shots (1 or 2) at once, each in its own "slot".
 //
 // Why: the one-shot kernel (relaybp_kernel.cuh) runs one 15-warp group per SM
 // for the benchmark code; its registers leave no room for a second group, so
@@ -47,10 +47,12 @@
 
 namespace rbpk {
 
-// Largest block an NS = 2 instantiation with VPT owned variables per thread is
-// compiled for (its register budget: two slots' posteriors and strengths).
-__host__ __device__ constexpr int max_slots_block_threads(int vpt) {
-  return vpt <= 4 ? 512 : (vpt == 6 ? 480 : (vpt == 8 ? 384 : (vpt == 12 ? 256 : 192)));
+// Largest block an instantiation with VPT owned variables per thread and NS
+// shots per group is compiled for (its register budget; two slots hold two
+// posteriors and strengths per variable).
+__host__ __device__ constexpr int max_slots_block_threads(int vpt, int ns = 2) {
+  return ns == 1 ? max_block_threads(vpt)
+                 : (vpt <= 4 ? 512 : (vpt == 6 ? 480 : (vpt == 8 ? 384 : (vpt == 12 ? 256 : 192))));
 }
 
 template <typename A, int VPT>
@@ -129,12 +131,13 @@ __device__ __forceinline__ void slot_check_row(M* msg, const M* first_tab, bool 
 }
 
 // Variable pass of one owned variable in one slot (kernels.py:1220-1350): memory
-// mix, posterior, new edge messages, hard decision; a flipped decision flips
-// its checks' mis bits and adds +-1 per check to dunsat.
-template <typename M, int MAXDC, int MAXDV>
-__device__ __forceinline__ void slot_var(M* msg, uint32_t* mis, const uint32_t (&vp)[MAXDV], uint32_t dummy, int kk,
-                                         typename MsgT<M>::A l0, typename MsgT<M>::A gam, int mix_mode,
-                                         typename MsgT<M>::A& post, uint32_t& hmask, int& dunsat, int VC) {
+// mix, posterior, new edge messages; returns the hard decision.  No branch: a
+// slot beyond the variable count has every edge on the dummy slot, a positive
+// prior and a positive posterior, so its decision stays 0.
+template <typename M, int MAXDV>
+__device__ __forceinline__ uint32_t slot_var(M* msg, const uint32_t (&vp)[MAXDV], uint32_t dummy,
+                                             typename MsgT<M>::A l0, typename MsgT<M>::A gam, int mix_mode,
+                                             typename MsgT<M>::A& post) {
   using IO = MsgT<M>;
   using A = typename IO::A;
   const A lm = memory_mix<A>(mix_mode, gam, l0, post);
@@ -149,19 +152,29 @@ __device__ __forceinline__ void slot_var(M* msg, uint32_t* mis, const uint32_t (
   post = pv;
 #pragma unroll
   for (int j = 0; j < MAXDV; ++j) msg[vp[j]] = IO::st(add_rn(lm, sub_rn(sum, nv[j])));
-  const uint32_t h = pv <= A(0) ? 1u : 0u;
-  if (h != ((hmask >> kk) & 1u)) {
-    hmask ^= 1u << kk;
+  return pv <= A(0) ? 1u : 0u;
+}
+
+// The variables in `flips` (bit k: variable t + k G) changed their hard decision:
+// flip their checks' mis bits and add +-1 per check to dunsat (the atomic's old
+// value says whether the check was unsatisfied).
+template <typename M, int MAXDC, int VPT, int MAXDV>
+__device__ __forceinline__ void slot_flips(uint32_t* mis, const uint32_t (&vpos)[VPT][MAXDV], uint32_t dummy,
+                                           uint32_t flips, int& dunsat, int VC) {
 #pragma unroll
-    for (int j = 0; j < MAXDV; ++j) {
-      uint32_t q = vp[j];
-      if (q != dummy) {
+  for (int kk = 0; kk < VPT; ++kk) {
+    if ((flips >> kk) & 1u) {
 #pragma unroll
-        for (int r = 1; r < MAXDC / VecIO<M>::N; ++r) q = q >= (uint32_t)VC ? q - (uint32_t)VC : q;
-        const uint32_t c = q / (uint32_t)VecIO<M>::N;
-        const uint32_t bit = 1u << (c & 31u);
-        const uint32_t old = atomicXor(mis + (c >> 5), bit);
-        dunsat += (old & bit) ? -1 : 1;
+      for (int j = 0; j < MAXDV; ++j) {
+        uint32_t q = vpos[kk][j];
+        if (q != dummy) {
+#pragma unroll
+          for (int r = 1; r < MAXDC / VecIO<M>::N; ++r) q = q >= (uint32_t)VC ? q - (uint32_t)VC : q;
+          const uint32_t c = q / (uint32_t)VecIO<M>::N;
+          const uint32_t bit = 1u << (c & 31u);
+          const uint32_t old = atomicXor(mis + (c >> 5), bit);
+          dunsat += (old & bit) ? -1 : 1;
+        }
       }
     }
   }
@@ -293,7 +306,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
 #pragma unroll
       for (int k = 0; k < VPT; ++k) {
         const int v = t + k * G;
-        x.post[k] = v < V ? sp[v] : A(0);
+        x.post[k] = v < V ? sp[v] : A(1);  // variable slots beyond V keep a positive posterior
       }
     } else {
       if (lane < VPT) {
@@ -306,7 +319,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
 #pragma unroll
       for (int k = 0; k < VPT; ++k) {
         const int v = t + k * G;
-        A p0 = A(0);
+        A p0 = A(1);  // variable slots beyond V keep a positive posterior
         if (v < V) {
           if (a.init_post) p0 = A(__ldg(a.init_post + b * (long long)V + v));
           else p0 = x.llr_row ? A(__ldg(x.llr_row + v)) : A(s_llr[v]);
@@ -569,16 +582,39 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
       fused = fused && st[s].run && !tab[s];
     }
     {
+      // ROWS owned rows per step (two for one slot): straight-line code with
+      // ROWS * NS independent chains when every slot computes
+      constexpr int ROWS = NS == 1 ? 2 : 1;
       int k = 0;
-      for (int c = t; c < C; c += G, ++k) {
-        const int deg = s_chk_deg[c];
+      for (; t + (k + ROWS - 1) * G < C; k += ROWS) {
         if (fused) {
-          // every slot computes: straight-line code, NS independent chains
 #pragma unroll
-          for (int s = 0; s < NS; ++s)
-            slot_check_row<M, MAXDC>(msg_of(s), first_tab, false, c, C, deg, (int)((st[s].synm >> k) & 1u),
-                                     alpha[s], a.use_alpha, a.use_beta, beta);
+          for (int r = 0; r < ROWS; ++r) {
+            const int c = t + (k + r) * G;
+            const int deg = s_chk_deg[c];
+#pragma unroll
+            for (int s = 0; s < NS; ++s)
+              slot_check_row<M, MAXDC>(msg_of(s), first_tab, false, c, C, deg, (int)((st[s].synm >> (k + r)) & 1u),
+                                       alpha[s], a.use_alpha, a.use_beta, beta);
+          }
         } else {
+#pragma unroll
+          for (int r = 0; r < ROWS; ++r) {
+            const int c = t + (k + r) * G;
+            const int deg = s_chk_deg[c];
+#pragma unroll
+            for (int s = 0; s < NS; ++s)
+              if (st[s].run)
+                slot_check_row<M, MAXDC>(msg_of(s), first_tab, tab[s], c, C, deg,
+                                         (int)((st[s].synm >> (k + r)) & 1u), alpha[s], a.use_alpha, a.use_beta,
+                                         beta);
+          }
+        }
+      }
+      if constexpr (ROWS > 1) {
+        if (t + k * G < C) {  // the last owned row when their number is odd
+          const int c = t + k * G;
+          const int deg = s_chk_deg[c];
 #pragma unroll
           for (int s = 0; s < NS; ++s)
             if (st[s].run)
@@ -597,30 +633,44 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
       dun[s] = 0;
       all_run = all_run && st[s].run;
     }
+    // Straight-line over the owned variables (and slots): the decisions are collected in a
+    // mask and the few flips handled after the loop, so no branch splits the loop body.
+    uint32_t hnew[NS];
 #pragma unroll
-    for (int kk = 0; kk < VPT; ++kk) {
+    for (int s = 0; s < NS; ++s) hnew[s] = 0u;
+    auto var_slot = [&](int s, int kk, A l0s) {
       const int v = t + kk * G;
-      if (v < V) {
-        const A l0s = A(s_llr[v]);
-        if (all_run) {
+      const A l0 = st[s].llr_row ? (v < V ? A(__ldg(st[s].llr_row + v)) : A(1)) : l0s;
+      hnew[s] |= slot_var<M, MAXDV>(msg_of(s), vpos[kk], dummy, l0, st[s].gam[kk], a.mix_mode, st[s].post[kk])
+                 << kk;
+    };
+    if (all_run) {
 #pragma unroll
-          for (int s = 0; s < NS; ++s)
-            slot_var<M, MAXDC, MAXDV>(msg_of(s), mis_of(s), vpos[kk], dummy, kk,
-                                      st[s].llr_row ? A(__ldg(st[s].llr_row + v)) : l0s, st[s].gam[kk], a.mix_mode,
-                                      st[s].post[kk], st[s].hmask, dun[s], VC);
-        } else {
+      for (int kk = 0; kk < VPT; ++kk) {
+        const int v = t + kk * G;
+        const A l0s = v < V ? A(s_llr[v]) : A(1);
 #pragma unroll
-          for (int s = 0; s < NS; ++s)
-            if (st[s].run)
-              slot_var<M, MAXDC, MAXDV>(msg_of(s), mis_of(s), vpos[kk], dummy, kk,
-                                        st[s].llr_row ? A(__ldg(st[s].llr_row + v)) : l0s, st[s].gam[kk],
-                                        a.mix_mode, st[s].post[kk], st[s].hmask, dun[s], VC);
+        for (int s = 0; s < NS; ++s) var_slot(s, kk, l0s);
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        if (!st[s].run) continue;
+#pragma unroll
+        for (int kk = 0; kk < VPT; ++kk) {
+          const int v = t + kk * G;
+          var_slot(s, kk, v < V ? A(s_llr[v]) : A(1));
         }
       }
     }
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-      if (dun[s] != 0) atomicAdd(unsat_of(s), dun[s]);
+      if (st[s].run) {
+        const uint32_t flips = hnew[s] ^ st[s].hmask;
+        st[s].hmask = hnew[s];
+        if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun[s], VC);
+        if (dun[s] != 0) atomicAdd(unsat_of(s), dun[s]);
+      }
       if (t == 0) red_of(s)[0] = 0;  // the next selection's sum; its last reader passed a barrier since
     }
     __syncthreads();
@@ -670,9 +720,9 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   }
 }
 
-// One code, NS shots per block (rbp_decode with shots_per_group 2).
+// One code, one group of NS shots per block (rbp_decode with groups_per_block 1).
 template <typename M, int MAXDC, int VPT, int MAXDV, int NS>
-__global__ void __launch_bounds__(max_slots_block_threads(VPT), 1)
+__global__ void __launch_bounds__(max_slots_block_threads(VPT, NS), 1)
 relaybp_slots_kernel(DevGraph g, DevArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   load_block_tables(g, a, smem);
@@ -681,34 +731,40 @@ relaybp_slots_kernel(DevGraph g, DevArgs a) {
   run_slots<M, MAXDC, VPT, MAXDV, NS>(g, a, smem);
 }
 
-KernelFn pick_slots_f32(int dc, int dv, int vpt);
-KernelFn pick_slots_f16(int dc, int dv, int vpt);
-KernelFn pick_slots_bf16(int dc, int dv, int vpt);
-KernelFn pick_slots_f64(int dc, int dv, int vpt);
+// Kernel for (check degree bound, variable degree, owned variables per thread,
+// shots per group 1 or 2), or null when this build has no such instantiation.
+KernelFn pick_slots_f32(int dc, int dv, int vpt, int ns);
+KernelFn pick_slots_f16(int dc, int dv, int vpt, int ns);
+KernelFn pick_slots_bf16(int dc, int dv, int vpt, int ns);
+KernelFn pick_slots_f64(int dc, int dv, int vpt, int ns);
 
 }  // namespace rbpk
 
-// Instantiation table of the two-slot kernel for one message type (check rows
-// of at most 8 or 16 slots; wider rows use the one-shot kernel).
-#define RBPK_SLOTS_DC_DV(M, DC, VPT)                                           \
-  if (dv <= 3) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 3, 2>;           \
-  if (dv <= 8) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 8, 2>;           \
+// Instantiation table of the block-per-group kernel for one message type
+// (check rows of at most 8 or 16 slots; wider rows use relaybp_decode_kernel).
+#define RBPK_SLOTS_DC_DV(M, DC, VPT, NS)                                       \
+  if (dv <= 3) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 3, NS>;          \
+  if (dv <= 8) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 8, NS>;          \
   return nullptr;
-#define RBPK_SLOTS_DC(M, VPT)                                                  \
-  if (dc <= 8) { RBPK_SLOTS_DC_DV(M, 8, VPT) }                                 \
-  if (dc <= 16) { RBPK_SLOTS_DC_DV(M, 16, VPT) }                               \
+#define RBPK_SLOTS_DC(M, VPT, NS)                                              \
+  if (dc <= 8) { RBPK_SLOTS_DC_DV(M, 8, VPT, NS) }                             \
+  if (dc <= 16) { RBPK_SLOTS_DC_DV(M, 16, VPT, NS) }                           \
   return nullptr;
+#define RBPK_SLOTS_VPT(M, NS)                                                  \
+  switch (vpt) {                                                               \
+    case 1: { RBPK_SLOTS_DC(M, 1, NS) }                                        \
+    case 2: { RBPK_SLOTS_DC(M, 2, NS) }                                        \
+    case 3: { RBPK_SLOTS_DC(M, 3, NS) }                                        \
+    case 4: { RBPK_SLOTS_DC(M, 4, NS) }                                        \
+    case 6: { RBPK_SLOTS_DC(M, 6, NS) }                                        \
+    case 8: { RBPK_SLOTS_DC(M, 8, NS) }                                        \
+    case 12: { RBPK_SLOTS_DC(M, 12, NS) }                                      \
+    case 16: { RBPK_SLOTS_DC(M, 16, NS) }                                      \
+    default: return nullptr;                                                   \
+  }
 #define RBPK_DEFINE_PICK_SLOTS(NAME, M)                                        \
-  rbpk::KernelFn rbpk::NAME(int dc, int dv, int vpt) {                         \
-    switch (vpt) {                                                             \
-      case 1: { RBPK_SLOTS_DC(M, 1) }                                          \
-      case 2: { RBPK_SLOTS_DC(M, 2) }                                          \
-      case 3: { RBPK_SLOTS_DC(M, 3) }                                          \
-      case 4: { RBPK_SLOTS_DC(M, 4) }                                          \
-      case 6: { RBPK_SLOTS_DC(M, 6) }                                          \
-      case 8: { RBPK_SLOTS_DC(M, 8) }                                          \
-      case 12: { RBPK_SLOTS_DC(M, 12) }                                        \
-      case 16: { RBPK_SLOTS_DC(M, 16) }                                        \
-      default: return nullptr;                                                 \
-    }                                                                          \
+  rbpk::KernelFn rbpk::NAME(int dc, int dv, int vpt, int ns) {                 \
+    if (ns == 1) { RBPK_SLOTS_VPT(M, 1) }                                      \
+    if (ns == 2) { RBPK_SLOTS_VPT(M, 2) }                                      \
+    return nullptr;                                                            \
   }

@@ -486,15 +486,18 @@ class RelayBPDecoder:
                                                return_last_posterior, prior_llr, leg_gammas)
             return self._decode_on(self.device_ids[0], syndromes, 0, pre, init_posterior, init_gamma,
                                    skip_relay_legs, return_last_posterior, prior_llr, leg_gammas)
+        # Replicas: every shard's kernels are enqueued on its own device before any result is
+        # read back (the reads synchronise the host), so the devices decode concurrently, as the
+        # reference's one host thread per GPU does (decoder.py:2475-2543).
         splits = self._split_batch(B, self.num_gpus)
-        parts = []
+        raws = []
         for gpu_id, (s0, s1) in zip(self.device_ids, splits):
             lg = leg_gammas[s0:s1] if leg_gammas is not None else None
             if self.hard_shots_first and self.num_sets > 0 and pre > 0 and s1 - s0 >= HARD_FIRST_MIN_BATCH:
-                parts.append(self._decode_hard_first(gpu_id, syndromes[s0:s1], pre, None, None, False, None, lg))
+                raws.append(self._launch_hard_first(gpu_id, syndromes[s0:s1], pre, None, None, False, None, lg))
             else:
-                parts.append(self._decode_on(gpu_id, syndromes[s0:s1], s0, pre, None, None, False, False,
-                                             None, lg))
+                raws.append(self._launch_on(gpu_id, syndromes[s0:s1], s0, pre, None, None, False, False, None, lg))
+        parts = [self._finish(r) for r in raws]
         return self._gather(parts, splits)
 
     @staticmethod
@@ -582,6 +585,12 @@ class RelayBPDecoder:
     def _decode_hard_first(self, gpu_id, syndromes, pre, init_posterior, init_gamma, return_last_posterior,
                            prior_llr, leg_gammas) -> Dict[str, torch.Tensor]:
         """Pre-iterations, then the relay legs with the unconverged shots queued first."""
+        return self._finish(self._launch_hard_first(gpu_id, syndromes, pre, init_posterior, init_gamma,
+                                                    return_last_posterior, prior_llr, leg_gammas))
+
+    def _launch_hard_first(self, gpu_id, syndromes, pre, init_posterior, init_gamma, return_last_posterior,
+                           prior_llr, leg_gammas) -> dict:
+        """_decode_hard_first's two launches, enqueued without a host synchronisation."""
         B = int(syndromes.shape[0])
         dev = self._device_strs[gpu_id]
         with torch.cuda.device(gpu_id):
@@ -591,14 +600,26 @@ class RelayBPDecoder:
                                     leg_gammas, None, state, 0, 0, light=True)
             # stable: converged shots (key 1) keep their order after the unconverged ones (key 0)
             order = torch.argsort((first["found_count"] > 0).to(torch.uint8), stable=True).to(torch.int32)
-            return self._decode_on(gpu_id, syn, 0, pre, None, None, False, return_last_posterior, prior_llr,
+            return self._launch_on(gpu_id, syn, 0, pre, None, None, False, return_last_posterior, prior_llr,
                                    leg_gammas, state, None, 0, 0, order=order)
 
     def _decode_on(self, gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
                    return_last_posterior, prior_llr, leg_gammas, resume=None, suspend=None, legs_begin=0,
                    legs_end=0, leg_gammas_legs=None, order=None, light=False) -> Dict[str, torch.Tensor]:
-        """One launch.  ``order`` sets the queue order; ``light`` returns only found_count and
-        iterations (no error rows, no host synchronisation)."""
+        """One launch and its result dict.  ``order`` sets the queue order; ``light`` returns only
+        found_count and iterations (no error rows, no host synchronisation)."""
+        raw = self._launch_on(gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
+                              return_last_posterior, prior_llr, leg_gammas, resume, suspend, legs_begin, legs_end,
+                              leg_gammas_legs, order, light)
+        if light:
+            return {"found_count": raw["found"], "iterations": raw["iters"]}
+        return self._finish(raw)
+
+    def _launch_on(self, gpu_id, syndromes, row0, pre, init_posterior, init_gamma, skip_relay_legs,
+                   return_last_posterior, prior_llr, leg_gammas, resume=None, suspend=None, legs_begin=0,
+                   legs_end=0, leg_gammas_legs=None, order=None, light=False) -> dict:
+        """Enqueue one decode launch on the device's current stream and return its output buffers
+        (no host synchronisation)."""
         B = int(syndromes.shape[0])
         dev = self._device_strs[gpu_id]
         with torch.cuda.device(gpu_id):
@@ -651,14 +672,21 @@ class RelayBPDecoder:
                                   last_posterior=_ptr(last_post))
             stream = torch.cuda.current_stream(gpu_id).cuda_stream
             self._native[gpu_id].decode(B, batch, outs, stream)
-            if light:
-                return {"found_count": found, "iterations": iters}
+            # Inputs freed after this call stay safe: the caching allocator reuses their memory
+            # only for work ordered after this stream's kernel.
+            return {"gpu_id": gpu_id, "found": found, "iters": iters, "wfix": wfix, "errors": errors,
+                    "packed": packed, "last_post": last_post}
+
+    def _finish(self, raw: dict) -> Dict[str, torch.Tensor]:
+        """The result dict of a launch's buffers (the unconverged-index list synchronises the host)."""
+        found, iters, wfix = raw["found"], raw["iters"], raw["wfix"]
+        with torch.cuda.device(raw["gpu_id"]):
             has = wfix != torch.iinfo(torch.int64).max
             wdt = torch.float64 if self.dtype_str == "float64" else torch.float32
             weights = torch.where(has, wfix.to(torch.float64) * (2.0 ** -32),
                                   torch.full_like(wfix, 0, dtype=torch.float64) + float("inf")).to(wdt)
             result = {
-                "errors": packed if self.bitpack_output else errors,
+                "errors": raw["packed"] if self.bitpack_output else raw["errors"],
                 "weights": weights,
                 "valid_mask": found >= self.stop_nconv,
                 "iterations": iters,
@@ -666,8 +694,6 @@ class RelayBPDecoder:
                 "unconverged_indices": torch.nonzero(found < self.stop_nconv).flatten().to(torch.int32),
                 "weight_fixed": wfix,
             }
-            if return_last_posterior:
-                result["last_posterior"] = last_post
-            # Inputs freed here stay safe: the caching allocator reuses their memory
-            # only for work ordered after this stream's kernel.
+            if raw["last_post"] is not None:
+                result["last_posterior"] = raw["last_post"]
             return result

@@ -286,6 +286,10 @@ def _cases():
         *bb144_phen(2, 0.004, 41),
         dict(pre_iter=6, num_sets=2, set_max_iter=4, gamma0=0.65, gamma_dist_interval=(-0.24, 0.66),
              stop_nconv=2, algo="relay", data_type="float32", seed=1234), {})
+    cases["bb144_phen_dense"] = lambda: (
+        *bb144_phen(2, 0.012, 43),
+        dict(pre_iter=12, num_sets=3, set_max_iter=6, gamma0=0.65, gamma_dist_interval=(-0.24, 0.66),
+             stop_nconv=3, algo="relay", data_type="float32", seed=1234), {})
     return cases
 
 
