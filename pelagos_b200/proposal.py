@@ -253,6 +253,11 @@ class LearnedRelayBPDecoder:
     after the bulk instead of beside it, which measured slower (21.7 vs 21.2 ms
     for 65,536 shots of the [[144,12,12]] phenomenological code).
 
+    ``network=False`` (gated only) is the ablation without the network: solved
+    shots still take ``hi`` on the learned legs, unconverged shots run the
+    seeded legs, and the network launch is skipped.  It separates what the
+    gate rule contributes from what the network contributes.
+
     With ``graph=True`` (default) the launches and the small device ops between
     them are captured once per batch size as a CUDA graph; a call then copies
     the syndromes into the captured input buffer and replays the graph.  Calls
@@ -265,7 +270,7 @@ class LearnedRelayBPDecoder:
     """
 
     def __init__(self, decoder: RelayBPDecoder, net: ProposalNet, learned_legs: int = 4, gate: bool = False,
-                 fused: bool = False, graph: bool = True):
+                 fused: bool = False, graph: bool = True, network: bool = True):
         if decoder.algo != "relay":
             raise ValueError("learned legs need algo='relay'")
         if decoder.num_gpus != 1:
@@ -274,6 +279,9 @@ class LearnedRelayBPDecoder:
         self.learned_legs = int(min(learned_legs, decoder.num_sets))
         self.lo, self.hi = (float(x) for x in decoder.gamma_dist_interval)
         self.gate = bool(gate)
+        self.network = bool(network)
+        if not self.network and not self.gate:
+            raise ValueError("network=False is the gate-only ablation: it needs gate=True")
         self.fused = bool(fused)
         self.graph = bool(graph)
         self._graphs: Dict[tuple, tuple] = {}  # (B, slot) -> (graph, static input, buffers)
@@ -348,13 +356,15 @@ class LearnedRelayBPDecoder:
         stride = bf["state"].shape[1] // 4
         if self.gate:
             # solved shots take the constant hi in the kernel; only unsolved rows are written
-            bf["count"].copy_(unsolved.sum().to(torch.int32).view(1))
-            self.net.propose_into(B, syn, post, self.lo, self.hi, bf["gammas"], order, bf["count"],
-                                  post_stride=stride)
+            if self.network:
+                bf["count"].copy_(unsolved.sum().to(torch.int32).view(1))
+                self.net.propose_into(B, syn, post, self.lo, self.hi, bf["gammas"], order, bf["count"],
+                                      post_stride=stride)
         else:
             self.net.propose_into(B, syn, post, self.lo, self.hi, bf["gammas"], post_stride=stride)
         legs_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter,
-                               gamma_legs_shot=_ptr(bf["gammas"]), n_shot_legs=self.learned_legs, shot_leg_rows=1,
+                               gamma_legs_shot=_ptr(bf["gammas"] if self.network else None),
+                               n_shot_legs=self.learned_legs if self.network else 0, shot_leg_rows=1,
                                resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order),
                                solved_gamma=float(np.float32(self.hi)),
                                solved_legs=self.learned_legs if self.gate else 0, parity_first=d.parity_first)
@@ -389,12 +399,14 @@ class LearnedRelayBPDecoder:
         order = torch.argsort((~unsolved).to(torch.uint8), stable=True).to(torch.int32)
         bf["count"].copy_(unsolved.sum().to(torch.int32).view(1))
         stride = bf["state"].shape[1]
-        self.net.propose_into(B, syn, bf["state"].data_ptr() + self._post_offset(), self.lo, self.hi,
-                              bf["gammas"], order, bf["count"], post_stride=stride // 4)
+        if self.network:
+            self.net.propose_into(B, syn, bf["state"].data_ptr() + self._post_offset(), self.lo, self.hi,
+                                  bf["gammas"], order, bf["count"], post_stride=stride // 4)
         if events is not None:
             events[2].record()
         legs_in = nat.RbpBatch(syndromes=_ptr(syn), gamma0=gamma0, pre_iter=d.pre_iter,
-                               gamma_legs_shot=_ptr(bf["gammas"]), n_shot_legs=self.learned_legs, shot_leg_rows=1,
+                               gamma_legs_shot=_ptr(bf["gammas"] if self.network else None),
+                               n_shot_legs=self.learned_legs if self.network else 0, shot_leg_rows=1,
                                resume_state=_ptr(bf["state"]), legs_begin=0, shot_order=_ptr(order),
                                queue_len=_ptr(bf["count"]))
         d._native[gid].decode(B, legs_in, outs, stream)
@@ -526,7 +538,8 @@ def constant_params(logit: float = 20.0) -> np.ndarray:
 
 
 def evaluate(workload, net: ProposalNet, decoder: RelayBPDecoder, shots: int, seed: int, chunk: int = 262144,
-             learned_legs: int = 4, variants=("plain", "learned", "learned_gated", "constant_hi")) -> dict:
+             learned_legs: int = 4,
+             variants=("plain", "learned", "learned_gated", "gate_no_network", "constant_hi")) -> dict:
     """Decode the same fresh seeded shots with each variant: logical error rate (Wilson 95% interval),
     mean iterations and decode time (device time, syndromes resident, one call per chunk).
 
@@ -534,6 +547,9 @@ def evaluate(workload, net: ProposalNet, decoder: RelayBPDecoder, shots: int, se
     learned        network strengths on legs 0..learned_legs-1 for every shot
     learned_gated  network strengths for the shots the pre-iterations left unconverged, the top
                    strength hi for the others
+    gate_no_network  the gate rule alone: hi on the learned legs for the shots the pre-iterations
+                   solved, the seeded legs for the others (no network): separates the rule from
+                   the network
     constant_hi    strength hi (a network with constant output) for every shot: the ablation
     """
     from .experiments import wilson
@@ -543,6 +559,7 @@ def evaluate(workload, net: ProposalNet, decoder: RelayBPDecoder, shots: int, se
         "plain": decoder.decode,
         "learned": LearnedRelayBPDecoder(decoder, net, learned_legs).decode,
         "learned_gated": LearnedRelayBPDecoder(decoder, net, learned_legs, gate=True).decode,
+        "gate_no_network": LearnedRelayBPDecoder(decoder, net, learned_legs, gate=True, network=False).decode,
         "constant_hi": LearnedRelayBPDecoder(decoder, const_net, learned_legs).decode,
     }
     rows = {v: {"fails": 0, "unconv": 0, "iters": 0, "ms": 0.0} for v in variants}

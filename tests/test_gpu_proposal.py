@@ -242,8 +242,14 @@ def test_trained_network_gains_over_seeded_legs():
     plain, f_plain = run(dec.decode)
     gated, f_gated = run(LearnedRelayBPDecoder(dec, net, gate=True).decode)
     const, f_const = run(LearnedRelayBPDecoder(dec, ProposalNet(dec, constant_params())).decode)
+    # the gate rule without the network: the solved shots' top strength, seeded legs for the rest
+    rule, f_rule = run(LearnedRelayBPDecoder(dec, net, gate=True, network=False).decode)
     assert gated["iterations"].mean() < 0.75 * plain["iterations"].mean()
     assert f_gated <= f_plain and f_gated < f_const, (f_gated, f_plain, f_const)
+    # what the network adds over the rule: the unconverged shots it solves
+    assert f_gated < f_rule, (f_gated, f_rule)
+    uns = (plain["found_count"] == 0) | (rule["found_count"] == 0)
+    assert (gated["found_count"][uns] > 0).sum() > (rule["found_count"][uns] > 0).sum()
     ok = gated["found_count"] > 0
     np.testing.assert_array_equal((w.H @ gated["errors"][ok].T.astype(np.int64) % 2).T, syn[ok])
 
