@@ -50,7 +50,8 @@ struct rbp_decoder {
   // launch shape
   KernelFn kernel = nullptr;
   int group_threads = 0, groups = 0, blocks = 0, vpt = 0;
-  int nshots = 1;              // shots a group decodes at once (2: relaybp_slots_kernel)
+  int nshots = 1;              // shots a group decodes at once
+  int slots_kernel = 0;        // 1: relaybp_slots_kernel (one group per block)
   int group_bytes = 0, block_bytes = 0;
   int sm_count = 0;
   size_t max_smem = 0;
@@ -166,7 +167,8 @@ cudaError_t set_max_dynamic_smem(const void* kernel, size_t max_smem, size_t* st
 struct Launch {
   KernelFn kernel;
   int group_threads, groups, blocks;
-  int nshots;  // shots a group decodes at once (relaybp_slots_kernel when groups == 1)
+  int nshots;        // shots a group decodes at once
+  int slots_kernel;  // 1: relaybp_slots_kernel (one group per block, nshots shot regions)
 };
 
 // Block-per-group shape: one group of G threads per block with nshots shot regions
@@ -192,7 +194,7 @@ int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_t
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G, smem));
   if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
-  *out = Launch{k, G, 1, per_sm * sm_count, nshots};
+  *out = Launch{k, G, 1, per_sm * sm_count, nshots, 1};
   return RBP_OK;
 }
 
@@ -236,7 +238,7 @@ int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, i
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * NG, smem));
   if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
-  *out = Launch{k, G, NG, per_sm * sm_count, 1};
+  *out = Launch{k, G, NG, per_sm * sm_count, 1, 0};
   return RBP_OK;
 }
 
@@ -451,6 +453,13 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
   const rbp_graph* g = d->g;
   const int nshots = shots_per_group > 0 ? shots_per_group : 1;
   const int G = group_threads > 0 ? group_threads : default_group_threads(g->C, g->V, nshots);
+  // Default: the block-per-group kernel where it exists (check degrees up to 16);
+  // -1: the multi-group kernel with as many one-shot groups per block as fit
+  if (groups_per_block == 0 && g->slots <= 16) groups_per_block = 1;
+  if (groups_per_block < 0) {
+    if (nshots != 1) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: groups_per_block -1 runs one shot per group");
+    groups_per_block = 0;
+  }
   DeviceGuard dg(g->device);
   Launch lc{};
   const int rc = choose_launch(g->C, g->V, g->slots, g->vslots, d->rows, d->p.msg_type, G, groups_per_block,
@@ -463,6 +472,7 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
   d->groups = lc.groups;
   d->blocks = lc.blocks;
   d->nshots = lc.nshots;
+  d->slots_kernel = lc.slots_kernel;
   d->group_bytes = L.group_bytes;
   d->block_bytes = L.off_group0;
   return RBP_OK;
@@ -575,7 +585,7 @@ int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs
   if (!dg.ok) return fail(RBP_ERR_CUDA, "rbp_decode: cannot select the CUDA device");
   const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, d->group_threads);
   const DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
-  const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks, d->nshots};
+  const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks, d->nshots, d->slots_kernel};
   return launch_decode(dgph, d->p, L, lc, d->llr.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
                        out, reinterpret_cast<cudaStream_t>(stream), "rbp_decode");
 }

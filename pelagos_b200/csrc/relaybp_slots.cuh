@@ -248,7 +248,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
 #pragma unroll
     for (int k = 0; k < VPT; ++k) {
       const int v = t + k * G;
-      if (v < V && x.post[k] <= A(0)) w += weight_units(x.llr_row ? __ldg(x.llr_row + v) : s_llr[v]);
+      if (v < V && ((x.hmask >> k) & 1u)) w += weight_units(x.llr_row ? __ldg(x.llr_row + v) : s_llr[v]);
     }
     return w;
   };
@@ -550,7 +550,88 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     }
   };
 
-  // ---------------------------------------------------------------- ticks
+  // ---------------------------------------------------------------- passes
+  // Check pass of slot x (c2v min-sum, or the first-pass table at a phase's first
+  // iteration), two owned rows per step so two rows' dependency chains interleave.
+  auto check_pass = [&](SlotState<A, VPT>& x, int s) {
+    const A alpha = a.use_alpha ? A(__ldg(a.alpha + x.it)) : A(1);
+    const bool tab = first_from_table && x.it == 0;
+    M* msg = msg_of(s);
+    int k = 0;
+    for (; t + (k + 1) * G < C; k += 2) {
+      const int c0 = t + k * G, c1 = c0 + G;
+      const int d0 = s_chk_deg[c0], d1 = s_chk_deg[c1];
+      slot_check_row<M, MAXDC>(msg, first_tab, tab, c0, C, d0, (int)((x.synm >> k) & 1u), alpha, a.use_alpha,
+                               a.use_beta, beta);
+      slot_check_row<M, MAXDC>(msg, first_tab, tab, c1, C, d1, (int)((x.synm >> (k + 1)) & 1u), alpha,
+                               a.use_alpha, a.use_beta, beta);
+    }
+    if (t + k * G < C)  // the last owned row when their number is odd
+      slot_check_row<M, MAXDC>(msg, first_tab, tab, t + k * G, C, s_chk_deg[t + k * G], (int)((x.synm >> k) & 1u),
+                               alpha, a.use_alpha, a.use_beta, beta);
+  };
+
+  // Variable pass of slot x, straight-line over the owned variables: the decisions are
+  // collected in a mask and the few flips applied after the loop, so no branch splits the
+  // loop body.  Ends with this thread's share of the unsatisfied-check count.
+  auto var_pass = [&](SlotState<A, VPT>& x, int s) {
+    M* msg = msg_of(s);
+    uint32_t hnew = 0u;
+#pragma unroll
+    for (int kk = 0; kk < VPT; ++kk) {
+      const int v = t + kk * G;
+      const A l0 = x.llr_row ? (v < V ? A(__ldg(x.llr_row + v)) : A(1)) : (v < V ? A(s_llr[v]) : A(1));
+      hnew |= slot_var<M, MAXDV>(msg, vpos[kk], dummy, l0, x.gam[kk], a.mix_mode, x.post[kk]) << kk;
+    }
+    const uint32_t flips = hnew ^ x.hmask;
+    x.hmask = hnew;
+    int dun = 0;
+    if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun, VC);
+    if (dun != 0) atomicAdd(unsat_of(s), dun);
+    if (t == 0) red_of(s)[0] = 0;  // the next selection's sum; its last reader passed a barrier since
+  };
+
+  // After slot x's variable pass and the barrier: the iteration's convergence test,
+  // selection and freeze.  Returns the slot's next event.
+  auto after_var = [&](SlotState<A, VPT>& x, int s) -> int {
+    x.it += 1;
+    const bool conv = *reinterpret_cast<volatile int*>(unsat_of(s)) == 0;
+    if (conv) {
+      // check_and_select_kernel (kernels.py:609-741): the weight sum and the test for
+      // decisions unchanged since the shot's last selection share one barrier
+      long long w = owned_weight(x);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+      if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(red_of(s)), (unsigned long long)w);
+      const bool differ = __syncthreads_or(x.hmask != x.hmask_sel) != 0;
+      if (!x.sel_seen || differ) {
+        // decisions equal to the last selection's have its weight: the best cannot change
+        x.hmask_sel = x.hmask;
+        x.sel_seen = true;
+        const long long tot = *reinterpret_cast<volatile long long*>(red_of(s));
+        if (!x.has_best || tot < x.best_w) {
+          x.best_w = tot;
+          x.has_best = true;
+          ballot_post<A, VPT>(x.post, best_of(s), warp, lane, G, V);
+        }
+      }
+      // freeze_finished_lanes_kernel (kernels.py:746-847): a convergence always freezes
+      x.found += 1;
+      x.iters += x.it;
+      x.hard_src = HARD_BEST;
+      x.run = false;
+      return EV_PHASE_DONE;
+    }
+    x.hard_src = HARD_POST;
+    if (x.it >= x.max_iter) {
+      x.iters += x.max_iter;
+      x.run = false;
+      return EV_PHASE_DONE;
+    }
+    return EV_NONE;
+  };
+
+  // ---------------------------------------------------------------- schedule
   // ev[s]: the event slot s has pending; every slot starts by claiming a shot.
   int ev[NS];
 #pragma unroll
@@ -562,158 +643,173 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     st[s].stopped = false;
     ev[s] = EV_SHOT_DONE;
   }
-  while (true) {
-    bool any = false;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      if (ev[s] != EV_NONE) events(st[s], s, ev[s]);
-      any = any || st[s].run;
+  if constexpr (NS == 1) {
+    // one shot: check pass, barrier, variable pass, barrier, events
+    while (true) {
+      if (ev[0] != EV_NONE) events(st[0], 0, ev[0]);
+      if (!st[0].run) break;
+      check_pass(st[0], 0);
+      __syncthreads();
+      var_pass(st[0], 0);
+      __syncthreads();
+      ev[0] = after_var(st[0], 0);
     }
-    if (!any) break;
+  } else {
+    // Two shots: one check pass of both slots (their rows interleaved), a barrier, one
+    // variable pass of both, a barrier, then each slot's events.
+    while (true) {
+      bool any = false;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        if (ev[s] != EV_NONE) events(st[s], s, ev[s]);
+        any = any || st[s].run;
+      }
+      if (!any) break;
 
-    // check pass of every running slot (c2v min-sum, or the first-pass table)
-    A alpha[NS];
-    bool tab[NS];
-    bool fused = true;
+      // check pass of every running slot (c2v min-sum, or the first-pass table)
+      A alpha[NS];
+      bool tab[NS];
+      bool fused = true;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      alpha[s] = (a.use_alpha && st[s].run) ? A(__ldg(a.alpha + st[s].it)) : A(1);
-      tab[s] = first_from_table && st[s].it == 0;
-      fused = fused && st[s].run && !tab[s];
-    }
-    {
-      // ROWS owned rows per step (two for one slot): straight-line code with
-      // ROWS * NS independent chains when every slot computes
-      constexpr int ROWS = NS == 1 ? 2 : 1;
-      int k = 0;
-      for (; t + (k + ROWS - 1) * G < C; k += ROWS) {
-        if (fused) {
+      for (int s = 0; s < NS; ++s) {
+        alpha[s] = (a.use_alpha && st[s].run) ? A(__ldg(a.alpha + st[s].it)) : A(1);
+        tab[s] = first_from_table && st[s].it == 0;
+        fused = fused && st[s].run && !tab[s];
+      }
+      {
+        // ROWS owned rows per step (two for one slot): straight-line code with
+        // ROWS * NS independent chains when every slot computes
+        constexpr int ROWS = NS == 1 ? 2 : 1;
+        int k = 0;
+        for (; t + (k + ROWS - 1) * G < C; k += ROWS) {
+          if (fused) {
 #pragma unroll
-          for (int r = 0; r < ROWS; ++r) {
-            const int c = t + (k + r) * G;
-            const int deg = s_chk_deg[c];
+            for (int r = 0; r < ROWS; ++r) {
+              const int c = t + (k + r) * G;
+              const int deg = s_chk_deg[c];
 #pragma unroll
-            for (int s = 0; s < NS; ++s)
-              slot_check_row<M, MAXDC>(msg_of(s), first_tab, false, c, C, deg, (int)((st[s].synm >> (k + r)) & 1u),
-                                       alpha[s], a.use_alpha, a.use_beta, beta);
+              for (int s = 0; s < NS; ++s)
+                slot_check_row<M, MAXDC>(msg_of(s), first_tab, false, c, C, deg, (int)((st[s].synm >> (k + r)) & 1u),
+                                         alpha[s], a.use_alpha, a.use_beta, beta);
+            }
+          } else {
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+              const int c = t + (k + r) * G;
+              const int deg = s_chk_deg[c];
+#pragma unroll
+              for (int s = 0; s < NS; ++s)
+                if (st[s].run)
+                  slot_check_row<M, MAXDC>(msg_of(s), first_tab, tab[s], c, C, deg,
+                                           (int)((st[s].synm >> (k + r)) & 1u), alpha[s], a.use_alpha, a.use_beta,
+                                           beta);
+            }
           }
-        } else {
-#pragma unroll
-          for (int r = 0; r < ROWS; ++r) {
-            const int c = t + (k + r) * G;
+        }
+        if constexpr (ROWS > 1) {
+          if (t + k * G < C) {  // the last owned row when their number is odd
+            const int c = t + k * G;
             const int deg = s_chk_deg[c];
 #pragma unroll
             for (int s = 0; s < NS; ++s)
               if (st[s].run)
-                slot_check_row<M, MAXDC>(msg_of(s), first_tab, tab[s], c, C, deg,
-                                         (int)((st[s].synm >> (k + r)) & 1u), alpha[s], a.use_alpha, a.use_beta,
-                                         beta);
+                slot_check_row<M, MAXDC>(msg_of(s), first_tab, tab[s], c, C, deg, (int)((st[s].synm >> k) & 1u),
+                                         alpha[s], a.use_alpha, a.use_beta, beta);
           }
         }
       }
-      if constexpr (ROWS > 1) {
-        if (t + k * G < C) {  // the last owned row when their number is odd
-          const int c = t + k * G;
-          const int deg = s_chk_deg[c];
-#pragma unroll
-          for (int s = 0; s < NS; ++s)
-            if (st[s].run)
-              slot_check_row<M, MAXDC>(msg_of(s), first_tab, tab[s], c, C, deg, (int)((st[s].synm >> k) & 1u),
-                                       alpha[s], a.use_alpha, a.use_beta, beta);
-        }
-      }
-    }
-    __syncthreads();
+      __syncthreads();
 
-    // variable pass of every running slot
-    int dun[NS];
-    bool all_run = true;
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      dun[s] = 0;
-      all_run = all_run && st[s].run;
-    }
-    // Straight-line over the owned variables (and slots): the decisions are collected in a
-    // mask and the few flips handled after the loop, so no branch splits the loop body.
-    uint32_t hnew[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) hnew[s] = 0u;
-    auto var_slot = [&](int s, int kk, A l0s) {
-      const int v = t + kk * G;
-      const A l0 = st[s].llr_row ? (v < V ? A(__ldg(st[s].llr_row + v)) : A(1)) : l0s;
-      hnew[s] |= slot_var<M, MAXDV>(msg_of(s), vpos[kk], dummy, l0, st[s].gam[kk], a.mix_mode, st[s].post[kk])
-                 << kk;
-    };
-    if (all_run) {
-#pragma unroll
-      for (int kk = 0; kk < VPT; ++kk) {
-        const int v = t + kk * G;
-        const A l0s = v < V ? A(s_llr[v]) : A(1);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) var_slot(s, kk, l0s);
-      }
-    } else {
+      // variable pass of every running slot
+      int dun[NS];
+      bool all_run = true;
 #pragma unroll
       for (int s = 0; s < NS; ++s) {
-        if (!st[s].run) continue;
+        dun[s] = 0;
+        all_run = all_run && st[s].run;
+      }
+      // Straight-line over the owned variables (and slots): the decisions are collected in a
+      // mask and the few flips handled after the loop, so no branch splits the loop body.
+      uint32_t hnew[NS];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) hnew[s] = 0u;
+      auto var_slot = [&](int s, int kk, A l0s) {
+        const int v = t + kk * G;
+        const A l0 = st[s].llr_row ? (v < V ? A(__ldg(st[s].llr_row + v)) : A(1)) : l0s;
+        hnew[s] |= slot_var<M, MAXDV>(msg_of(s), vpos[kk], dummy, l0, st[s].gam[kk], a.mix_mode, st[s].post[kk])
+                   << kk;
+      };
+      if (all_run) {
 #pragma unroll
         for (int kk = 0; kk < VPT; ++kk) {
           const int v = t + kk * G;
-          var_slot(s, kk, v < V ? A(s_llr[v]) : A(1));
+          const A l0s = v < V ? A(s_llr[v]) : A(1);
+#pragma unroll
+          for (int s = 0; s < NS; ++s) var_slot(s, kk, l0s);
         }
-      }
-    }
+      } else {
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      if (st[s].run) {
-        const uint32_t flips = hnew[s] ^ st[s].hmask;
-        st[s].hmask = hnew[s];
-        if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun[s], VC);
-        if (dun[s] != 0) atomicAdd(unsat_of(s), dun[s]);
-      }
-      if (t == 0) red_of(s)[0] = 0;  // the next selection's sum; its last reader passed a barrier since
-    }
-    __syncthreads();
-
-    // the iteration's convergence test, selection and freeze, per slot
+        for (int s = 0; s < NS; ++s) {
+          if (!st[s].run) continue;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      SlotState<A, VPT>& x = st[s];
-      ev[s] = EV_NONE;
-      if (!x.run) continue;
-      x.it += 1;
-      const bool conv = *reinterpret_cast<volatile int*>(unsat_of(s)) == 0;
-      if (conv) {
-        // check_and_select_kernel (kernels.py:609-741): the weight sum and the test for
-        // decisions unchanged since the shot's last selection share one barrier
-        long long w = owned_weight(x);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-        if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(red_of(s)), (unsigned long long)w);
-        const bool differ = __syncthreads_or(x.hmask != x.hmask_sel) != 0;
-        if (!x.sel_seen || differ) {
-          // decisions equal to the last selection's have its weight: the best cannot change
-          x.hmask_sel = x.hmask;
-          x.sel_seen = true;
-          const long long tot = *reinterpret_cast<volatile long long*>(red_of(s));
-          if (!x.has_best || tot < x.best_w) {
-            x.best_w = tot;
-            x.has_best = true;
-            ballot_post<A, VPT>(x.post, best_of(s), warp, lane, G, V);
+          for (int kk = 0; kk < VPT; ++kk) {
+            const int v = t + kk * G;
+            var_slot(s, kk, v < V ? A(s_llr[v]) : A(1));
           }
         }
-        // freeze_finished_lanes_kernel (kernels.py:746-847): a convergence always freezes
-        x.found += 1;
-        x.iters += x.it;
-        x.hard_src = HARD_BEST;
-        x.run = false;
-        ev[s] = EV_PHASE_DONE;
-      } else {
-        x.hard_src = HARD_POST;
-        if (x.it >= x.max_iter) {
-          x.iters += x.max_iter;
+      }
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        if (st[s].run) {
+          const uint32_t flips = hnew[s] ^ st[s].hmask;
+          st[s].hmask = hnew[s];
+          if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun[s], VC);
+          if (dun[s] != 0) atomicAdd(unsat_of(s), dun[s]);
+        }
+        if (t == 0) red_of(s)[0] = 0;  // the next selection's sum; its last reader passed a barrier since
+      }
+      __syncthreads();
+
+      // the iteration's convergence test, selection and freeze, per slot
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        SlotState<A, VPT>& x = st[s];
+        ev[s] = EV_NONE;
+        if (!x.run) continue;
+        x.it += 1;
+        const bool conv = *reinterpret_cast<volatile int*>(unsat_of(s)) == 0;
+        if (conv) {
+          // check_and_select_kernel (kernels.py:609-741): the weight sum and the test for
+          // decisions unchanged since the shot's last selection share one barrier
+          long long w = owned_weight(x);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+          if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(red_of(s)), (unsigned long long)w);
+          const bool differ = __syncthreads_or(x.hmask != x.hmask_sel) != 0;
+          if (!x.sel_seen || differ) {
+            // decisions equal to the last selection's have its weight: the best cannot change
+            x.hmask_sel = x.hmask;
+            x.sel_seen = true;
+            const long long tot = *reinterpret_cast<volatile long long*>(red_of(s));
+            if (!x.has_best || tot < x.best_w) {
+              x.best_w = tot;
+              x.has_best = true;
+              ballot_post<A, VPT>(x.post, best_of(s), warp, lane, G, V);
+            }
+          }
+          // freeze_finished_lanes_kernel (kernels.py:746-847): a convergence always freezes
+          x.found += 1;
+          x.iters += x.it;
+          x.hard_src = HARD_BEST;
           x.run = false;
           ev[s] = EV_PHASE_DONE;
+        } else {
+          x.hard_src = HARD_POST;
+          if (x.it >= x.max_iter) {
+            x.iters += x.max_iter;
+            x.run = false;
+            ev[s] = EV_PHASE_DONE;
+          }
         }
       }
     }

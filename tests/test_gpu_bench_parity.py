@@ -5,8 +5,9 @@ phenomenological workload at p = 0.003 (seed 2026), full Relay-BP-S schedule
 (pre 80, 100 legs x 60, gamma0 0.65, U(-0.24, 0.66), stop_nconv 5), float32 —
 decoded on the GPU and compared bit for bit with the CPU oracle:
 
-* the plain decoder (RelayBPDecoder.decode), with both kernels (one and two
-  shots per group);
+* the plain decoder (RelayBPDecoder.decode), with every kernel family (the
+  block-per-group kernel with one and with two shots per group, and the kernel
+  whose blocks hold several one-shot groups);
 * the gated learned decoder (LearnedRelayBPDecoder, gate=True) against the
   oracle's per-shot emulation of it: shots the pre-iterations solved run relay
   legs 0-3 at the constant top strength, the others run them with the
@@ -73,23 +74,23 @@ def plain_oracle(bench_batch):
     return _oracle_chunks(dec, syn, dec._leg_table(0))
 
 
-@pytest.mark.parametrize("nshots", [1, 2])
+@pytest.mark.parametrize("nshots", [(0, 1), (0, 2), (-1, 1)])
 def test_plain_decode_of_the_bench_batch_matches_oracle(bench_batch, plain_oracle, nshots):
     w, syn = bench_batch
-    dec = RelayBPDecoder(w.H, w.priors, launch=(0, 0, nshots), **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, launch=(0, *nshots), **RELAY)
     out = dec.decode(torch.from_numpy(syn).to(DEV))
     got = {k: out[k].cpu().numpy() for k in KEYS}
-    _assert_same(got, plain_oracle, f"plain decode, {nshots} shot(s) per group")
+    _assert_same(got, plain_oracle, f"plain decode, launch {nshots}")
     # the long relay tails are exercised
     assert got["iterations"].max() > 200
 
 
-@pytest.mark.parametrize("nshots", [1, 2])
+@pytest.mark.parametrize("nshots", [(0, 1), (0, 2), (-1, 1)])
 def test_gated_learned_decode_of_the_bench_batch_matches_oracle_emulation(bench_batch, nshots):
     from pelagos_b200.proposal import LearnedRelayBPDecoder, ProposalNet, default_weights_path, load_params
 
     w, syn = bench_batch
-    dec = RelayBPDecoder(w.H, w.priors, launch=(0, 0, nshots), **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, launch=(0, *nshots), **RELAY)
     net = ProposalNet(dec, load_params(default_weights_path("bb144_phen", P))[0])
     learned = LearnedRelayBPDecoder(dec, net, learned_legs=4, gate=True, graph=False)
     syn_d = torch.from_numpy(syn).to(DEV)
@@ -113,4 +114,4 @@ def test_gated_learned_decode_of_the_bench_batch_matches_oracle_emulation(bench_
     for k in KEYS:
         want[k][sol] = r_sol[k]
         want[k][uns] = r_uns[k]
-    _assert_same(got, want, f"gated learned decode, {nshots} shot(s) per group")
+    _assert_same(got, want, f"gated learned decode, launch {nshots}")

@@ -52,16 +52,17 @@ def _golden_decode_kwargs(g):
     return d
 
 
-#: shots a group decodes at once: the one-shot kernel and the two-shot kernel
-NSHOTS = [1, 2]
+#: kernel families, as (groups_per_block, shots_per_group): the block-per-group kernel with one
+#: and with two shots per group, and the kernel whose blocks hold several one-shot groups
+NSHOTS = [(0, 1), (0, 2), (-1, 1)]
 
 
 @pytest.mark.parametrize("nshots", NSHOTS)
 def test_reference_fixtures_bit_exact(golden, nshots):
     try:
-        dec = _golden_decoder(golden, launch=(0, 0, nshots))
+        dec = _golden_decoder(golden, launch=(0, *nshots))
     except NotImplementedError:
-        if nshots == 1:
+        if nshots[1] == 1:
             raise
         pytest.skip("the two-shot kernel covers check degrees up to 16")
     out = _np(dec.decode(torch.from_numpy(golden.syndromes).to(DEV), **_golden_decode_kwargs(golden)))
@@ -101,7 +102,7 @@ def _assert_same(out, ref, keys=KEYS):
 def test_bb72_code_capacity_matches_oracle(dtype, nshots):
     w = codes.workload("bb72_cc")
     err, syn = w.sample(1024 if dtype == "float32" else 256, seed=7)
-    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, launch=(0, 0, nshots), **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, launch=(0, *nshots), **RELAY)
     out = _np(dec.decode(torch.from_numpy(syn).to(DEV), return_last_posterior=True))
     ref = _oracle_for(dec, syn)
     _assert_same(out, ref)
@@ -113,7 +114,7 @@ def test_bb72_code_capacity_matches_oracle(dtype, nshots):
 def test_bb144_phenomenological_matches_oracle(dtype, nshots):
     w = codes.workload("bb144_phen")
     err, syn = w.sample(384, seed=11)
-    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, launch=(0, 0, nshots), **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, data_type=dtype, launch=(0, *nshots), **RELAY)
     out = _np(dec.decode(torch.from_numpy(syn).to(DEV)))
     _assert_same(out, _oracle_for(dec, syn))
 
@@ -133,7 +134,7 @@ def test_options_match_oracle(variant, nshots):
     kw.update(pre_iter=20, num_sets=12, set_max_iter=15)
     mix = variant.pop("mix_rounding", "separate")
     kw.update(variant)
-    dec = RelayBPDecoder(w.H, w.priors, mix_rounding=mix, launch=(0, 0, nshots), **kw)
+    dec = RelayBPDecoder(w.H, w.priors, mix_rounding=mix, launch=(0, *nshots), **kw)
     out = _np(dec.decode(torch.from_numpy(syn).to(DEV)))
     _assert_same(out, _oracle_for(dec, syn, mix=mix))
 
@@ -149,7 +150,7 @@ def test_per_shot_inputs_match_oracle(nshots):
     pl = rng.uniform(2.5, 4.5, (256, V)).astype(np.float32)
     lg = rng.uniform(-0.24, 0.66, (256, 3, V)).astype(np.float32)
     kw = dict(RELAY, pre_iter=25, num_sets=8, set_max_iter=20, stop_nconv=3)
-    dec = RelayBPDecoder(w.H, w.priors, launch=(0, 0, nshots), **kw)
+    dec = RelayBPDecoder(w.H, w.priors, launch=(0, *nshots), **kw)
     t = lambda a: torch.from_numpy(a).to(DEV)  # noqa: E731
     out = _np(dec.decode(t(syn), init_posterior=t(ip), init_gamma=t(ig), prior_llr=t(pl), leg_gammas=t(lg),
                          pre_iter_override=30, return_last_posterior=True))
