@@ -142,10 +142,10 @@ int vpt_for(int V, int G) {
 // Default shape: the fewest owned variables per thread (from 3 up) whose group
 // still fits the register budget of that count (of the one- or two-shot
 // kernel), so a shot's iteration is short.
-int default_group_threads(int C, int V, int nshots = 1) {
+int default_group_threads(int C, int V, int nshots = 1, int vslots = 8) {
   for (int vpt : {3, 4, 6, 8, 12, 16}) {
     const int G = std::max(32, (V + vpt - 1) / vpt + 31) / 32 * 32;
-    const int max_threads = rbpk::max_slots_block_threads(vpt, nshots);
+    const int max_threads = rbpk::max_slots_block_threads(vpt, nshots, vslots <= 3 ? 3 : 8);
     if (G <= max_threads && (C + G - 1) / G <= 32 && vpt_for(V, G) <= vpt) return G;
   }
   return 256;  // configure reports why no shape fits
@@ -176,7 +176,7 @@ struct Launch {
 int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int nshots,
                         size_t max_smem, int sm_count, Launch* out, const std::string& w) {
   const int vpt = vpt_for(V, G);
-  const int max_threads = rbpk::max_slots_block_threads(vpt, nshots);
+  const int max_threads = rbpk::max_slots_block_threads(vpt, nshots, vslots <= 3 ? 3 : 8);
   if (G > max_threads)
     return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +
                                          " variables each exceed the register budget of " + std::to_string(nshots) +
@@ -452,7 +452,6 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: null decoder");
   const rbp_graph* g = d->g;
   const int nshots = shots_per_group > 0 ? shots_per_group : 1;
-  const int G = group_threads > 0 ? group_threads : default_group_threads(g->C, g->V, nshots);
   // Default: the block-per-group kernel where it exists (check degrees up to 16);
   // -1: the multi-group kernel with as many one-shot groups per block as fit
   if (groups_per_block == 0 && g->slots <= 16) groups_per_block = 1;
@@ -460,6 +459,10 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
     if (nshots != 1) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: groups_per_block -1 runs one shot per group");
     groups_per_block = 0;
   }
+  const bool block_per_group = nshots == 2 || groups_per_block == 1;
+  // default group size within the register budget of the kernel family that runs it
+  const int G = group_threads > 0 ? group_threads
+                                  : default_group_threads(g->C, g->V, nshots, block_per_group ? g->vslots : 8);
   DeviceGuard dg(g->device);
   Launch lc{};
   const int rc = choose_launch(g->C, g->V, g->slots, g->vslots, d->rows, d->p.msg_type, G, groups_per_block,

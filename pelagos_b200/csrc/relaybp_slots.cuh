@@ -50,7 +50,8 @@ namespace rbpk {
 // Largest block an instantiation with VPT owned variables per thread and NS
 // shots per group is compiled for (its register budget; two slots hold two
 // posteriors and strengths per variable).
-__host__ __device__ constexpr int max_slots_block_threads(int vpt, int ns = 2) {
+__host__ __device__ constexpr int max_slots_block_threads(int vpt, int ns = 2, int maxdv = 3) {
+  (void)maxdv;  // the same budget for 3- and 8-edge variables
   return ns == 1 ? max_block_threads(vpt)
                  : (vpt <= 4 ? 512 : (vpt == 6 ? 480 : (vpt == 8 ? 384 : (vpt == 12 ? 256 : 192))));
 }
@@ -818,7 +819,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
 
 // One code, one group of NS shots per block (rbp_decode with groups_per_block 1).
 template <typename M, int MAXDC, int VPT, int MAXDV, int NS>
-__global__ void __launch_bounds__(max_slots_block_threads(VPT, NS), 1)
+__global__ void __launch_bounds__(max_slots_block_threads(VPT, NS, MAXDV), 1)
 relaybp_slots_kernel(DevGraph g, DevArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   load_block_tables(g, a, smem);
