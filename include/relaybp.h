@@ -240,6 +240,13 @@ RBP_API int rbp_mixed_replay(rbp_mixed* m, void* stream);
 RBP_API int rbp_mixed_query(const rbp_mixed* m, int32_t i, int32_t* group_threads, int32_t* groups_per_block,
                             int32_t* block_threads, int32_t* blocks);
 
+/* Set each code's group size inside the mixed launch (group_threads[i]; 0 keeps
+ * code i's current size): a multiple of 32 that divides the launch's block size
+ * and leaves each thread at most the instantiation's variables and 32 checks.
+ * Each code gets as many groups per block as fit.  Drops a captured graph.
+ * The autotuner's hook; no reference counterpart. */
+RBP_API int rbp_mixed_configure(rbp_mixed* m, const int32_t* group_threads);
+
 /* Size of the scratch array that rbp_decode_static uses (1 MiB per GPU). */
 #define RBP_STATIC_SCRATCH_BYTES (1 << 20)
 

@@ -49,6 +49,7 @@ EXPORTED_SYMBOLS = (
     "rbp_mixed_capture",
     "rbp_mixed_replay",
     "rbp_mixed_query",
+    "rbp_mixed_configure",
     "rbp_net_param_count",
     "rbp_net_create",
     "rbp_net_destroy",
@@ -191,6 +192,8 @@ def _declare(lib):
     lib.rbp_mixed_replay.argtypes = [P, P]
     lib.rbp_mixed_query.restype = ct.c_int
     lib.rbp_mixed_query.argtypes = [P, i32, i32p, i32p, i32p, i32p]
+    lib.rbp_mixed_configure.restype = ct.c_int
+    lib.rbp_mixed_configure.argtypes = [P, ct.POINTER(i32)]
     lib.rbp_net_param_count.restype = ct.c_int
     lib.rbp_net_param_count.argtypes = [ct.POINTER(i64)]
     lib.rbp_net_create.restype = ct.c_int

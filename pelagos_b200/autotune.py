@@ -151,3 +151,38 @@ def tune(dec, syndromes: torch.Tensor, shapes: Optional[Iterable[Tuple[int, ...]
     _store(key, {"shape": list(shape), "ms": ms, "sample_shots": B,
                  "tried": [[list(s), t] for t, s in sorted(results)]})
     return shape
+
+
+def tune_mixed(mix, syndromes, repeats: int = 3, rounds: int = 2, verbose: bool = False) -> List[int]:
+    """Per-code group sizes of a mixed launch (``MixedDecoder``): coordinate descent, one code
+    at a time over the group sizes the launch's block size allows (multiples of 32 dividing it;
+    the library rejects sizes whose threads would own too many variables or checks), each
+    candidate timed as the median of ``repeats`` decodes of ``syndromes`` (one batch per code).
+    Configures and returns the fastest sizes."""
+    T = mix.launch_info()[0]["block_threads"]
+    shapes = [x["group_threads"] for x in mix.launch_info()]
+    best = _time(lambda: mix.decode(syndromes), repeats)
+    if verbose:
+        print(f"  start {shapes}: {best:8.3f} ms", flush=True)
+    for _ in range(rounds):
+        improved = False
+        for i in range(len(shapes)):
+            for G in range(32, T + 1, 32):
+                if T % G or G == shapes[i]:
+                    continue
+                trial = list(shapes)
+                trial[i] = G
+                try:
+                    mix.configure(trial)
+                except (NotImplementedError, ValueError):
+                    continue
+                ms = _time(lambda: mix.decode(syndromes), repeats)
+                if verbose:
+                    print(f"  {trial}: {ms:8.3f} ms", flush=True)
+                if ms < best:
+                    best, shapes, improved = ms, trial, True
+            mix.configure(shapes)
+        if not improved:
+            break
+    mix.configure(shapes)
+    return shapes

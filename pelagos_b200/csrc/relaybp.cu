@@ -603,6 +603,7 @@ struct rbp_mixed {
   const rbp_decoder* dec[rbpk::kMaxMixedCodes] = {};
   int G[rbpk::kMaxMixedCodes] = {}, NG[rbpk::kMaxMixedCodes] = {};
   rbpk::MixedKernelFn kernel = nullptr;
+  int vpt = 0;                 // owned variables per thread of the instantiation
   int block_threads = 0, blocks = 0;
   size_t smem = 0;
   DevBuf<int> queues;
@@ -784,6 +785,7 @@ int rbp_mixed_create(const rbp_decoder* const* decoders, int32_t n, rbp_mixed** 
       return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_create: no mixed kernel for these degrees");
     }
     m->block_threads = T;
+    m->vpt = vpt;
     m->smem = smem;
     break;
   }
@@ -869,6 +871,55 @@ int rbp_mixed_query(const rbp_mixed* m, int32_t i, int32_t* group_threads, int32
   if (groups_per_block) *groups_per_block = m->NG[i];
   if (block_threads) *block_threads = m->block_threads;
   if (blocks) *blocks = m->blocks;
+  return RBP_OK;
+}
+
+// Per-code group sizes of a mixed launch (autotuner hook; no reference counterpart).
+int rbp_mixed_configure(rbp_mixed* m, const int32_t* group_threads) {
+  if (!m || !group_threads) return fail(RBP_ERR_ARGUMENT, "rbp_mixed_configure: null argument");
+  const int T = m->block_threads;
+  int G[rbpk::kMaxMixedCodes], NG[rbpk::kMaxMixedCodes];
+  size_t smem = 0;
+  for (int i = 0; i < m->n; ++i) {
+    const rbp_decoder* d = m->dec[i];
+    const rbp_graph* g = d->g;
+    const int Gi = group_threads[i] > 0 ? group_threads[i] : m->G[i];
+    if (Gi % 32 || T % Gi)
+      return fail(RBP_ERR_ARGUMENT, "rbp_mixed_configure: code " + std::to_string(i) + ": " + std::to_string(Gi) +
+                                        " threads must be a multiple of 32 dividing the block's " +
+                                        std::to_string(T));
+    const int need = vpt_for(g->V, Gi);
+    if (need < 0 || need > m->vpt || (g->C + Gi - 1) / Gi > 32)
+      return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_configure: code " + std::to_string(i) + ": " +
+                                           std::to_string(Gi) + " threads own more than " + std::to_string(m->vpt) +
+                                           " variables or 32 checks each");
+    const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, Gi);
+    int ng = std::min(T / Gi, Gi == 32 ? T / Gi : 15);
+    while (ng >= 1 && (size_t)L.off_group0 + (size_t)ng * L.group_bytes > d->max_smem) --ng;
+    if (ng < 1)
+      return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_configure: code " + std::to_string(i) + ": no group fits");
+    G[i] = Gi;
+    NG[i] = ng;
+    smem = std::max(smem, (size_t)L.off_group0 + (size_t)ng * L.group_bytes);
+  }
+  DeviceGuard dg(m->device);
+  int per_sm = 0;
+  RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m->kernel, T, smem));
+  if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, "rbp_mixed_configure: zero occupancy");
+  for (int i = 0; i < m->n; ++i) {
+    m->G[i] = G[i];
+    m->NG[i] = NG[i];
+  }
+  m->smem = smem;
+  m->blocks = per_sm * m->dec[0]->sm_count;
+  if (m->exec) {  // a captured graph holds the old shapes
+    cudaGraphExecDestroy(m->exec);
+    m->exec = nullptr;
+  }
+  if (m->graph) {
+    cudaGraphDestroy(m->graph);
+    m->graph = nullptr;
+  }
   return RBP_OK;
 }
 

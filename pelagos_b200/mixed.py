@@ -59,6 +59,15 @@ class MixedDecoder:
                         "blocks": b.value})
         return out
 
+    def configure(self, group_threads: Sequence[int]) -> None:
+        """Set each code's group size in the launch (0 keeps a code's current size); the next
+        decode re-captures its graph."""
+        if len(group_threads) != len(self.decoders):
+            raise ValueError(f"expected {len(self.decoders)} group sizes")
+        arr = (ct.c_int32 * len(group_threads))(*[int(g) for g in group_threads])
+        nat.check(nat.lib().rbp_mixed_configure(self._m, arr), "rbp_mixed_configure")
+        self._captured = None
+
     def _alloc(self, sizes: Tuple[int, ...]):
         dev = f"cuda:{self.device}"
         self._bufs = []

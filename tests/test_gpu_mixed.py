@@ -78,3 +78,37 @@ def test_autotune_keeps_results(tmp_path, monkeypatch):
     assert autotune.lookup(dec, 2048) == shape  # cached
     dec2 = RelayBPDecoder(w.H, w.priors, **RELAY)
     assert autotune.tune(dec2, syn) == shape  # served from the cache
+
+
+def test_mixed_launch_matches_oracle():
+    """Each code's shots from one mixed launch, bit for bit against the CPU oracle (a few hundred
+    shots per code; the oracle restates the reference loop per shot)."""
+    from oracle import oracle as O
+
+    decs, syns, hosts = [], [], []
+    for i, (name, p) in enumerate(MIX):
+        w = codes.workload(name, p=p)
+        dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+        syn = w.sample(256, seed=70 + i)[1]
+        decs.append(dec)
+        syns.append(torch.from_numpy(syn).to(DEV))
+        hosts.append(syn)
+    outs = [_np(o) for o in MixedDecoder(decs, graph=True).decode(syns)]
+    for (name, p), dec, syn, o in zip(MIX, decs, hosts, outs):
+        ref = O.decode(O.reference_graph(dec.H_csr), syn, dec.log_prior_ratios, pre_iter=dec.pre_iter,
+                       num_sets=dec.num_sets, set_max_iter=dec.set_max_iter, stop_nconv=dec.stop_nconv,
+                       gamma0=dec.gamma0, gamma_legs=dec._leg_table(0))
+        for k in ("errors", "found_count", "iterations", "weight_fixed"):
+            np.testing.assert_array_equal(o[k], ref[k], err_msg=f"{name} {k}")
+
+
+def test_mixed_autotune_keeps_results(mixed_case):
+    """Per-code group sizes chosen by the mixed autotuner change no result."""
+    decs, syns, singles = mixed_case
+    mix = MixedDecoder(decs, graph=True)
+    shapes = autotune.tune_mixed(mix, syns, repeats=1, rounds=1)
+    assert [x["group_threads"] for x in mix.launch_info()] == shapes
+    outs = [_np(o) for o in mix.decode(syns)]
+    for name_p, o, ref in zip(MIX, outs, singles):
+        for k in KEYS:
+            np.testing.assert_array_equal(o[k], ref[k], err_msg=f"{name_p} {k}")
