@@ -431,6 +431,8 @@ def main():
                       "roofline": {"bound": "smem", "achieved": p_achieved, "peak": smem_peak, "unit": "GB/s",
                                    "frac": p_achieved / smem_peak, "shot_iterations_per_step": p_iters},
                       "note": "the same shots through RelayBPDecoder.decode (seeded legs), same run"},
+            "step_ms": {"learned": {"min": min(l_steps), "median": float(np.median(l_steps)), "max": max(l_steps)},
+                        "plain": {"min": min(p_steps), "median": float(np.median(p_steps)), "max": max(p_steps)}},
             "learned_over_plain": p_ms / ms_step,
             "phase_ms": {"decode_kernel": kern, "network_and_selection": float(np.mean(net_ms)),
                          "note": "eager runs of the same decode with events between its launches"},
@@ -488,6 +490,11 @@ def run_mixed(args) -> None:
         ws.append(w)
         errs.append(err)
     mix = MixedDecoder(decs, graph=True)
+    tuned = None
+    if args.autotune:
+        from pelagos_b200 import autotune
+
+        tuned = autotune.tune_mixed(mix, syns, repeats=3)
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         mix.decode(syns)
@@ -522,7 +529,7 @@ def run_mixed(args) -> None:
         "data": "synthetic (seeded i.i.d. Bernoulli errors, s = H e mod 2)",
         "config": {"workload": "262,144 shots: [[72,12,6]] cc p=0.03, [[144,12,12]] cc p=0.03, "
                                "[[144,12,12]] phenomenological p=0.003, (3,6)-regular 2000x4000 p=0.02",
-                   "launch": mix.launch_info()},
+                   "launch": mix.launch_info(), "autotuned_group_threads": tuned},
         "separate_launches": {"ms_per_step": ms_seq, "shots_per_s": 262144 / (ms_seq / 1000.0)},
         "per_code": per_code, "gpu_launches": args.steps,
     }
