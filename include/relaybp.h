@@ -109,10 +109,9 @@ RBP_API int rbp_decoder_set_llr(rbp_decoder* d, const float* llr);
  * `group_threads` threads (a multiple of 32, at most 1024) decodes
  * `shots_per_group` shots at once (1 or 2) and a thread block holds
  * `groups_per_block` such groups.  groups_per_block 1, or two shots per
- * group, selects the block-per-group kernel (check degrees up to 16); other
- * counts the kernel whose blocks hold several one-shot groups (groups_per_block
- * 0 with check degrees up to 16 means 1; -1 asks for that kernel with as many
- * groups as fit).  Zeros pick the defaults.  Results do not depend on the shape.  Fails with
+ * group, selects the block-per-group kernel (check degrees up to 16); 0 (or
+ * -1) the kernel whose blocks hold as many one-shot groups as fit.  Zeros pick
+ * the defaults.  Results do not depend on the shape.  Fails with
  * RBP_ERR_UNSUPPORTED when the shape's registers or shared memory do not fit. */
 RBP_API int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block,
                                   int32_t shots_per_group);

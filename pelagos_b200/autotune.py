@@ -13,9 +13,9 @@ the reference keys its tuning cache (src/pelagos/autotune.py:130-133, 222-541):
 
 * cache file: ``$PELAGOS_B200_TUNE_CACHE`` or ``~/.cache/pelagos_b200_tune.json``;
 * candidates: every warp multiple G from 32 to 1024 that gives at most 16
-  variables and 32 checks per thread, each with the largest group count that
-  fits (and, for one-warp groups, also half of it), and the same G values for
-  two-shot groups;
+  variables and 32 checks per thread, with the multi-group kernel (the largest
+  group count that fits and, for one-warp groups, also 8) and with the
+  block-per-group kernel (one and two shots per group);
 * a candidate the library rejects (shared memory, registers) is skipped.
 
 ``default_shape`` returns the shape measured best for a workload and
@@ -79,9 +79,11 @@ def candidates(C: int, V: int) -> List[Tuple[int, int, int]]:
             need = -(-V // G)
             if need > 16 or -(-C // G) > 32:
                 continue
-            out.append((G, 0 if ns == 1 else 1, ns))
-            if G == 32 and ns == 1:
-                out.append((G, 8, 1))
+            if ns == 1:
+                out.append((G, 0, 1))   # several one-shot groups per block, as many as fit
+                if G == 32:
+                    out.append((G, 8, 1))
+            out.append((G, 1, ns))      # the block-per-group kernel
     return out
 
 

@@ -452,9 +452,8 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: null decoder");
   const rbp_graph* g = d->g;
   const int nshots = shots_per_group > 0 ? shots_per_group : 1;
-  // Default: the block-per-group kernel where it exists (check degrees up to 16);
-  // -1: the multi-group kernel with as many one-shot groups per block as fit
-  if (groups_per_block == 0 && g->slots <= 16) groups_per_block = 1;
+  // groups_per_block 0 (default) or -1: the multi-group kernel with as many one-shot groups
+  // per block as fit; 1, or two shots per group: the block-per-group kernel
   if (groups_per_block < 0) {
     if (nshots != 1) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: groups_per_block -1 runs one shot per group");
     groups_per_block = 0;

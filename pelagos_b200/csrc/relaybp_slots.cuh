@@ -45,6 +45,8 @@
 
 #include "relaybp_kernel.cuh"
 
+#include <type_traits>
+
 namespace rbpk {
 
 // Largest block an instantiation with VPT owned variables per thread and NS
@@ -135,13 +137,14 @@ __device__ __forceinline__ void slot_check_row(M* msg, const M* first_tab, bool 
 // mix, posterior, new edge messages; returns the hard decision.  No branch: a
 // slot beyond the variable count has every edge on the dummy slot, a positive
 // prior and a positive posterior, so its decision stays 0.
-template <typename M, int MAXDV>
+template <typename M, int MAXDV, bool STORE = true>
 __device__ __forceinline__ uint32_t slot_var(M* msg, const uint32_t (&vp)[MAXDV], uint32_t dummy,
                                              typename MsgT<M>::A l0, typename MsgT<M>::A gam, int mix_mode,
-                                             typename MsgT<M>::A& post) {
+                                             typename MsgT<M>::A& post, typename MsgT<M>::A* lm_out = nullptr) {
   using IO = MsgT<M>;
   using A = typename IO::A;
   const A lm = memory_mix<A>(mix_mode, gam, l0, post);
+  if (lm_out) *lm_out = lm;
   A nv[MAXDV];
   A sum = A(0);
 #pragma unroll
@@ -151,9 +154,30 @@ __device__ __forceinline__ uint32_t slot_var(M* msg, const uint32_t (&vp)[MAXDV]
   }
   const A pv = add_rn(lm, sum);
   post = pv;
+  if constexpr (STORE) {
+#pragma unroll
+    for (int j = 0; j < MAXDV; ++j) msg[vp[j]] = IO::st(add_rn(lm, sub_rn(sum, nv[j])));
+  }
+  return pv <= A(0) ? 1u : 0u;
+}
+
+// The variable-to-check messages of a variable pass that skipped them (slot_var with
+// STORE false): the incoming messages are reloaded (still in their slots) and summed in
+// the same order, so the values are those the pass would have stored.
+template <typename M, int MAXDV>
+__device__ __forceinline__ void slot_var_store(M* msg, const uint32_t (&vp)[MAXDV], uint32_t dummy,
+                                               typename MsgT<M>::A lm) {
+  using IO = MsgT<M>;
+  using A = typename IO::A;
+  A nv[MAXDV];
+  A sum = A(0);
+#pragma unroll
+  for (int j = 0; j < MAXDV; ++j) {
+    nv[j] = IO::ld(msg[vp[j]]);
+    sum = (vp[j] != dummy) ? add_rn(sum, nv[j]) : sum;
+  }
 #pragma unroll
   for (int j = 0; j < MAXDV; ++j) msg[vp[j]] = IO::st(add_rn(lm, sub_rn(sum, nv[j])));
-  return pv <= A(0) ? 1u : 0u;
 }
 
 // The variables in `flips` (bit k: variable t + k G) changed their hard decision:
@@ -575,14 +599,20 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   // Variable pass of slot x, straight-line over the owned variables: the decisions are
   // collected in a mask and the few flips applied after the loop, so no branch splits the
   // loop body.  Ends with this thread's share of the unsatisfied-check count.
-  auto var_pass = [&](SlotState<A, VPT>& x, int s) {
+  // With DEFER the outgoing messages are not stored (see the one-shot schedule below);
+  // the memory mixes are kept in lm_keep for slot_var_store.
+  A lm_keep[VPT];
+  auto var_pass = [&](SlotState<A, VPT>& x, int s, auto defer) {
+    constexpr bool DEFER = decltype(defer)::value;
     M* msg = msg_of(s);
     uint32_t hnew = 0u;
 #pragma unroll
     for (int kk = 0; kk < VPT; ++kk) {
       const int v = t + kk * G;
       const A l0 = x.llr_row ? (v < V ? A(__ldg(x.llr_row + v)) : A(1)) : (v < V ? A(s_llr[v]) : A(1));
-      hnew |= slot_var<M, MAXDV>(msg, vpos[kk], dummy, l0, x.gam[kk], a.mix_mode, x.post[kk]) << kk;
+      hnew |= slot_var<M, MAXDV, !DEFER>(msg, vpos[kk], dummy, l0, x.gam[kk], a.mix_mode, x.post[kk],
+                                         DEFER ? &lm_keep[kk] : nullptr)
+              << kk;
     }
     const uint32_t flips = hnew ^ x.hmask;
     x.hmask = hnew;
@@ -651,9 +681,20 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
       if (!st[0].run) break;
       check_pass(st[0], 0);
       __syncthreads();
-      var_pass(st[0], 0);
+      // A relay leg's first iteration usually converges (most legs of solved shots repeat
+      // their solution), and then its outgoing messages are never read: the next leg restarts
+      // them.  Those passes store them only once the iteration is known not to have converged.
+      const bool defer = st[0].phase >= 0 && st[0].it == 0;
+      if (defer) var_pass(st[0], 0, std::true_type{});
+      else var_pass(st[0], 0, std::false_type{});
       __syncthreads();
       ev[0] = after_var(st[0], 0);
+      if (defer && st[0].run) {
+        M* msg = msg_of(0);
+#pragma unroll
+        for (int kk = 0; kk < VPT; ++kk) slot_var_store<M, MAXDV>(msg, vpos[kk], dummy, lm_keep[kk]);
+        __syncthreads();  // the next check pass reads them
+      }
     }
   } else {
     // Two shots: one check pass of both slots (their rows interleaved), a barrier, one

@@ -53,8 +53,8 @@ def _golden_decode_kwargs(g):
 
 
 #: kernel families, as (groups_per_block, shots_per_group): the block-per-group kernel with one
-#: and with two shots per group, and the kernel whose blocks hold several one-shot groups
-NSHOTS = [(0, 1), (0, 2), (-1, 1)]
+#: and with two shots per group, and the (default) kernel whose blocks hold several one-shot groups
+NSHOTS = [(1, 1), (1, 2), (0, 1)]
 
 
 @pytest.mark.parametrize("nshots", NSHOTS)
@@ -62,9 +62,9 @@ def test_reference_fixtures_bit_exact(golden, nshots):
     try:
         dec = _golden_decoder(golden, launch=(0, *nshots))
     except NotImplementedError:
-        if nshots[1] == 1:
+        if nshots == (0, 1):
             raise
-        pytest.skip("the two-shot kernel covers check degrees up to 16")
+        pytest.skip("the block-per-group kernel covers check degrees up to 16")
     out = _np(dec.decode(torch.from_numpy(golden.syndromes).to(DEV), **_golden_decode_kwargs(golden)))
     z = golden.z
     np.testing.assert_array_equal(out["errors"], z["out_errors"])
