@@ -73,6 +73,7 @@ struct SlotState {
   float gs;
   int phase, it, max_iter, found, iters, hard_src;
   int claim;            // which red[1 + claim] entry the next claim writes
+  int wsel;             // one-shot kernel: the next selection sums into red[0] (0) or red[4] (1)
   bool run, has_best, sel_seen, solved_pre, stopped;
 };
 
@@ -257,7 +258,11 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     for (int w = t; w < Wc; w += G) mis_of(s)[w] = 0u;
-    if (t == 0) *unsat_of(s) = 0;
+    if (t == 0) {
+      *unsat_of(s) = 0;
+      red_of(s)[0] = 0;
+      red_of(s)[4] = 0;
+    }
   }
   __syncthreads();
 
@@ -619,7 +624,6 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     int dun = 0;
     if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun, VC);
     if (dun != 0) atomicAdd(unsat_of(s), dun);
-    if (t == 0) red_of(s)[0] = 0;  // the next selection's sum; its last reader passed a barrier since
   };
 
   // After slot x's variable pass and the barrier: the iteration's convergence test,
@@ -630,22 +634,28 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     if (conv) {
       // check_and_select_kernel (kernels.py:609-741): the weight sum and the test for
       // decisions unchanged since the shot's last selection share one barrier
+      // The sum goes to red[0] or red[4], alternating: once this selection's barrier has
+      // passed, the other entry's last readers (the previous selection's) are done and thread 0
+      // clears it, so no pass between two selections has to.
+      long long* wsum = red_of(s) + (x.wsel ? 4 : 0);
       long long w = owned_weight(x);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-      if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(red_of(s)), (unsigned long long)w);
+      if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(wsum), (unsigned long long)w);
       const bool differ = __syncthreads_or(x.hmask != x.hmask_sel) != 0;
+      if (t == 0) red_of(s)[x.wsel ? 0 : 4] = 0;
       if (!x.sel_seen || differ) {
         // decisions equal to the last selection's have its weight: the best cannot change
         x.hmask_sel = x.hmask;
         x.sel_seen = true;
-        const long long tot = *reinterpret_cast<volatile long long*>(red_of(s));
+        const long long tot = *reinterpret_cast<volatile long long*>(wsum);
         if (!x.has_best || tot < x.best_w) {
           x.best_w = tot;
           x.has_best = true;
           ballot_post<A, VPT>(x.post, best_of(s), warp, lane, G, V);
         }
       }
+      x.wsel ^= 1;
       // freeze_finished_lanes_kernel (kernels.py:746-847): a convergence always freezes
       x.found += 1;
       x.iters += x.it;
@@ -668,6 +678,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     st[s].claim = 0;
+    st[s].wsel = 0;
     st[s].run = false;
     st[s].b = -1;  // no shot yet: the first EV_SHOT_DONE only claims
     st[s].has_best = false;
