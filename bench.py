@@ -39,6 +39,7 @@ batch (weak scaling, no collective on the data path).
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -312,10 +313,14 @@ def main():
     def timed_steps(fn):
         """K steps, each between its own pair of events on the launching stream; the L2 flush between
         steps (a 256 MB write) lies outside them.  The region is bracketed by a barrier and a device
-        synchronisation on both sides; ms per step is the mean over steps, max over ranks."""
+        synchronisation on both sides; ms per step is the mean over steps, max over ranks.  Python's
+        garbage collector is paused inside it: a collection between a step's first event and its
+        launch would leave the GPU idle inside the step."""
         for _ in range(args.warmup):
             fn()
             flush.zero_()
+        gc.collect()
+        gc.disable()
         barrier()
         step_ev = [[ev(), ev()] for _ in range(args.steps)]
         step_iters, o = [], None
@@ -326,6 +331,7 @@ def main():
             step_ev[k][1].record(stream)
             step_iters.append(o["iterations"])  # only the counts are kept across steps
         barrier()
+        gc.enable()
         per_step = [a.elapsed_time(b) for a, b in step_ev]
         ms = max_over_ranks(float(np.mean(per_step)), pg, dev)
         iters = sum(int(it.sum().item()) for it in step_iters) / args.steps
@@ -366,17 +372,22 @@ def main():
     batches = [syn_pin] * e2e_steps
     outs = [ring[i % 2] for i in range(e2e_steps)]
     learned.decode_stream(batches[:2], outs[:2])  # warm-up: the second buffer set's graph
+    gc.collect()
+    gc.disable()
     barrier()
     e0, e1 = ev(), ev()
     e0.record(stream)
     learned.decode_stream(batches, outs)
     e1.record(stream)
     barrier()
+    gc.enable()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps, pg, dev)
     e2e_value = whole_job_shots_per_s(world, shots, e2e_ms)
     # (b) one decode() call per batch, its results copied to pinned host memory before the next
     res_pin = ring[0]
     call_steps = max(1, min(args.steps, 10))
+    gc.collect()
+    gc.disable()
     barrier()
     c0, c1 = ev(), ev()
     c0.record(stream)
@@ -386,6 +397,7 @@ def main():
             t.copy_(o[k], non_blocking=True)
     c1.record(stream)
     barrier()
+    gc.enable()
     call_ms = max_over_ranks(c0.elapsed_time(c1) / call_steps, pg, dev)
 
     if rank == 0:
