@@ -31,9 +31,10 @@
 // Shared memory: the block tables (relaybp_kernel.cuh), then NS slot regions
 // of `group_bytes` each laid out like the one-shot kernel's group region:
 // messages, mis bits, best bits, first-leg bits, and `red`:
-//   red[0] weight sum of a selection, red[1..2] the claimed shot index (two
-//   entries used in turn, so a claim never overwrites one a thread has not read
-//   yet), red[3] (int) the count of unsatisfied checks.
+//   red[0] weight sum of a selection (one-shot groups alternate it with red[4]),
+//   red[1..2] the claimed shot index (two entries used in turn, so a claim never
+//   overwrites one a thread has not read yet), red[3] (int) the count of
+//   unsatisfied checks.
 //
 // Bit-set words are "owned" by the warp whose threads own their bits: thread
 // t = 32 w + l owns variables t + k G, whose bits sit in word w + k (G/32) at
