@@ -633,20 +633,29 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     x.it += 1;
     const bool conv = *reinterpret_cast<volatile int*>(unsat_of(s)) == 0;
     if (conv) {
-      // check_and_select_kernel (kernels.py:609-741): the weight sum and the test for
-      // decisions unchanged since the shot's last selection share one barrier
-      // The sum goes to red[0] or red[4], alternating: once this selection's barrier has
-      // passed, the other entry's last readers (the previous selection's) are done and thread 0
-      // clears it, so no pass between two selections has to.
+      // check_and_select_kernel (kernels.py:609-741).  Decisions equal to the shot's last
+      // selection's have its weight, so the best cannot change: after the shot's first selection
+      // the "decisions differ" test comes first (one OR-barrier) and the weight sum, with a second
+      // barrier, only when they do.  The sum goes to red[0] or red[4], alternating: once a
+      // selection's sum barrier has passed, the other entry's last readers (the previous
+      // selection's) are done and thread 0 clears it, so no pass between two selections has to.
       long long* wsum = red_of(s) + (x.wsel ? 4 : 0);
-      long long w = owned_weight(x);
+      auto add_weight = [&]() {
+        long long w = owned_weight(x);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-      if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(wsum), (unsigned long long)w);
-      const bool differ = __syncthreads_or(x.hmask != x.hmask_sel) != 0;
-      if (t == 0) red_of(s)[x.wsel ? 0 : 4] = 0;
-      if (!x.sel_seen || differ) {
-        // decisions equal to the last selection's have its weight: the best cannot change
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (lane == 0 && w != 0) atomicAdd(reinterpret_cast<unsigned long long*>(wsum), (unsigned long long)w);
+        __syncthreads();
+      };
+      bool select = true;
+      if (x.sel_seen) {
+        select = __syncthreads_or(x.hmask != x.hmask_sel) != 0;
+        if (select) add_weight();
+      } else {
+        add_weight();
+      }
+      if (select) {
+        if (t == 0) red_of(s)[x.wsel ? 0 : 4] = 0;
         x.hmask_sel = x.hmask;
         x.sel_seen = true;
         const long long tot = *reinterpret_cast<volatile long long*>(wsum);
@@ -655,8 +664,8 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
           x.has_best = true;
           ballot_post<A, VPT>(x.post, best_of(s), warp, lane, G, V);
         }
+        x.wsel ^= 1;
       }
-      x.wsel ^= 1;
       // freeze_finished_lanes_kernel (kernels.py:746-847): a convergence always freezes
       x.found += 1;
       x.iters += x.it;
