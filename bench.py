@@ -252,7 +252,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--shots", type=int, default=SHOTS)
     ap.add_argument("--launch", default=None,
-                    help="G,groups[,shots_per_group]: kernel shape (default: the committed shape of this workload)")
+                    help="G,groups[,shots_per_group[,blocks_per_sm]]: kernel shape of every launch "
+                         "(default: the committed shapes of this workload)")
     ap.add_argument("--autotune", action="store_true",
                     help="time the candidate shapes on the learned decode (the measured path) first")
     ap.add_argument("--workload", default="bb144_phen", choices=["bb144_phen", "mixed"])
@@ -289,9 +290,7 @@ def main():
     launch = tuple(int(x) for x in args.launch.split(",")) if args.launch else None
     dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], launch=launch, **RELAY)
     if launch is None:
-        shape = autotune.default_shape(dec)  # the shape committed for this workload, if any
-        if shape is not None:
-            dec.configure_launch(*shape)
+        autotune.apply_default_shapes(dec)  # the shapes committed for this workload, if any
     params, meta = load_params(default_weights_path(WORKLOAD, P))
     learned = LearnedRelayBPDecoder(dec, ProposalNet(dec, params), learned_legs=LEARNED_LEGS, gate=True)
     syn_dev = torch.from_numpy(syn).to(dev)

@@ -112,16 +112,46 @@ RBP_API int rbp_decoder_set_llr(rbp_decoder* d, const float* llr);
  * group, selects the block-per-group kernel (check degrees up to 16); 0 (or
  * -1) the kernel whose blocks hold as many one-shot groups as fit.  Zeros pick
  * the defaults.  Results do not depend on the shape.  Fails with
- * RBP_ERR_UNSUPPORTED when the shape's registers or shared memory do not fit. */
+ * RBP_ERR_UNSUPPORTED when the shape's registers or shared memory do not fit.
+ * Sets the shape of every launch kind (rbp_decoder_configure_kind with
+ * RBP_LAUNCH_ALL and one resident block per SM). */
 RBP_API int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block,
                                   int32_t shots_per_group);
 
+/* Launch kinds.  A decode launch whose rbp_batch.skip_relay_legs is set runs
+ * the pre-iterations only, so no shot runs more than pre_iter iterations in
+ * it; such launches use the RBP_LAUNCH_PRE shape, every other launch the
+ * RBP_LAUNCH_LEGS shape. */
+#define RBP_LAUNCH_ALL 0
+#define RBP_LAUNCH_PRE 1
+#define RBP_LAUNCH_LEGS 2
+
+/* Launch shape of one launch kind (no reference counterpart, like
+ * rbp_decoder_configure).  blocks_per_sm 2 selects the block-per-group kernel
+ * compiled for two resident blocks per SM (groups_per_block 1 and
+ * shots_per_group 1 only; half the register file per block, so
+ * group_threads is at most 512 for up to 4 owned variables per thread, 480
+ * for 6, 384 for 8 and 256 for 12 or 16): two shots decode side by side on an
+ * SM, each at a longer iteration latency, which raises throughput and can
+ * lengthen a batch whose slowest shot bounds it.  0 or 1: the kernels compiled
+ * for one resident block.  Results do not depend on the shape. */
+RBP_API int rbp_decoder_configure_kind(rbp_decoder* d, int32_t kind, int32_t group_threads,
+                                       int32_t groups_per_block, int32_t shots_per_group,
+                                       int32_t blocks_per_sm);
+
 /* Shared-memory bytes of one shot's region and of the block-wide tables for
- * the current message type; the shape currently configured.  Any pointer may
- * be NULL. */
+ * the current message type; the RBP_LAUNCH_LEGS shape currently configured.
+ * Any pointer may be NULL. */
 RBP_API int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem,
                       int32_t* group_threads, int32_t* groups_per_block, int32_t* blocks,
                       int32_t* shots_per_group);
+
+/* The shape configured for launch kind RBP_LAUNCH_PRE or RBP_LAUNCH_LEGS;
+ * blocks_per_sm is the resident-block count the kernel is compiled for and
+ * blocks the persistent grid.  Any pointer may be NULL. */
+RBP_API int rbp_decoder_query_kind(const rbp_decoder* d, int32_t kind, int32_t* group_threads,
+                                   int32_t* groups_per_block, int32_t* shots_per_group,
+                                   int32_t* blocks_per_sm, int32_t* blocks);
 
 /* Per-call inputs (device memory).  Optional pointers may be NULL.
  * Mirrors decode()'s keyword arguments (src/pelagos/decoder.py:2317-2361).

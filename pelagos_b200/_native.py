@@ -28,6 +28,10 @@ RBP_MIX_SEPARATE = 0
 RBP_MIX_FMA_GP = 1
 RBP_MIX_FMA_LP = 2
 
+RBP_LAUNCH_ALL = 0
+RBP_LAUNCH_PRE = 1
+RBP_LAUNCH_LEGS = 2
+
 #: Every symbol include/relaybp.h declares.
 EXPORTED_SYMBOLS = (
     "rbp_last_error",
@@ -39,6 +43,8 @@ EXPORTED_SYMBOLS = (
     "rbp_decoder_set_llr",
     "rbp_decoder_configure",
     "rbp_decoder_query",
+    "rbp_decoder_configure_kind",
+    "rbp_decoder_query_kind",
     "rbp_state_bytes",
     "rbp_state_posterior_offset",
     "rbp_decode",
@@ -170,6 +176,10 @@ def _declare(lib):
     lib.rbp_decoder_configure.argtypes = [P, i32, i32, i32]
     lib.rbp_decoder_query.restype = ct.c_int
     lib.rbp_decoder_query.argtypes = [P, ct.POINTER(i64), ct.POINTER(i64), i32p, i32p, i32p, i32p]
+    lib.rbp_decoder_configure_kind.restype = ct.c_int
+    lib.rbp_decoder_configure_kind.argtypes = [P, i32, i32, i32, i32, i32]
+    lib.rbp_decoder_query_kind.restype = ct.c_int
+    lib.rbp_decoder_query_kind.argtypes = [P, i32, i32p, i32p, i32p, i32p, i32p]
     lib.rbp_state_bytes.restype = ct.c_int
     lib.rbp_state_bytes.argtypes = [P, ct.POINTER(i64)]
     lib.rbp_state_posterior_offset.restype = ct.c_int

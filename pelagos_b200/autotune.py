@@ -1,10 +1,13 @@
 """Launch-shape autotuner for the decode kernel.
 
-The kernel's shape is (group_threads, groups_per_block, shots_per_group): how
-many threads share one shot (and so how many variables and checks each thread
-owns), how many groups a thread block holds, and how many shots a group
-decodes at once (1: relaybp_decode_kernel; 2: relaybp_slots_kernel, one group
-per block).  ``tune`` times candidate shapes on a sample batch with CUDA events
+The kernel's shape is (group_threads, groups_per_block, shots_per_group[,
+blocks_per_sm]): how many threads share one shot (and so how many variables
+and checks each thread owns), how many groups a thread block holds, how many
+shots a group decodes at once (1: relaybp_decode_kernel; 2: relaybp_slots_kernel,
+one group per block), and for one-shot block-per-group launches how many
+blocks the kernel is compiled to keep resident per SM (2: half the register
+file each, two shots side by side with their own barriers).  The launches
+that run only the pre-iterations may have their own shape (``kind="pre"``).  ``tune`` times candidate shapes on a sample batch with CUDA events
 (the median of ``repeats`` timed runs after a warm-up, by default of
 ``decoder.decode`` and optionally of any decode call, e.g. a learned decode)
 and keeps the fastest.  The choice is cached in a JSON file keyed by device
@@ -15,13 +18,16 @@ the reference keys its tuning cache (src/pelagos/autotune.py:130-133, 222-541):
 * candidates: every warp multiple G from 32 to 1024 that gives at most 16
   variables and 32 checks per thread, with the multi-group kernel (the largest
   group count that fits and, for one-warp groups, also 8) and with the
-  block-per-group kernel (one and two shots per group);
+  block-per-group kernel (one and two shots per group, and one shot per group
+  at two resident blocks per SM);
 * a candidate the library rejects (shared memory, registers) is skipped.
 
 ``default_shape`` returns the shape measured best for a workload and
 committed with the package (``data/launch_shapes.json``, keyed by graph
-sparsity hash and message type), so a fresh machine starts from a measured
-shape instead of re-tuning on a noisy sample.
+sparsity hash and message type; ``default_pre_shape`` the pre-iteration
+launches' shape where the entry gives one, and ``apply_default_shapes``
+configures both), so a fresh machine starts from a measured shape instead of
+re-tuning on a noisy sample.
 """
 
 from __future__ import annotations
@@ -84,6 +90,8 @@ def candidates(C: int, V: int) -> List[Tuple[int, int, int]]:
                 if G == 32:
                     out.append((G, 8, 1))
             out.append((G, 1, ns))      # the block-per-group kernel
+            if ns == 1 and G <= 512:
+                out.append((G, 1, 1, 2))  # the same, compiled for two resident blocks per SM
     return out
 
 
@@ -95,14 +103,36 @@ def lookup(dec, B: int) -> Optional[Tuple[int, ...]]:
 SHAPES_FILE = Path(__file__).resolve().parent / "data" / "launch_shapes.json"
 
 
-def default_shape(dec) -> Optional[Tuple[int, int, int]]:
-    """The committed shape for this graph and message type, or None."""
+def _committed(dec) -> Optional[dict]:
     try:
         table = json.loads(SHAPES_FILE.read_text())
     except (OSError, ValueError):
         return None
-    v = table.get(f"{dec.graph.sparsity_hash}|{dec.dtype_str}")
+    return table.get(f"{dec.graph.sparsity_hash}|{dec.dtype_str}")
+
+
+def default_shape(dec) -> Optional[Tuple[int, ...]]:
+    """The committed shape for this graph and message type, or None."""
+    v = _committed(dec)
     return tuple(v["shape"]) if v else None
+
+
+def default_pre_shape(dec) -> Optional[Tuple[int, ...]]:
+    """The committed shape of the pre-iteration launches, or None (they use ``default_shape``)."""
+    v = _committed(dec)
+    return tuple(v["pre_shape"]) if v and "pre_shape" in v else None
+
+
+def apply_default_shapes(dec) -> bool:
+    """Configure the committed shapes of this workload; False when none is committed."""
+    shape = default_shape(dec)
+    if shape is None:
+        return False
+    dec.configure_launch(*shape)
+    pre = default_pre_shape(dec)
+    if pre is not None:
+        dec.configure_launch(*pre, kind="pre")
+    return True
 
 
 def _time(fn: Callable[[], object], repeats: int) -> float:
@@ -122,12 +152,13 @@ def _time(fn: Callable[[], object], repeats: int) -> float:
 
 def tune(dec, syndromes: torch.Tensor, shapes: Optional[Iterable[Tuple[int, ...]]] = None, repeats: int = 5,
          use_cache: bool = True, verbose: bool = False,
-         decode_fn: Optional[Callable[[torch.Tensor], object]] = None) -> Tuple[int, ...]:
+         decode_fn: Optional[Callable[[torch.Tensor], object]] = None, kind: str = "all") -> Tuple[int, ...]:
     """Time the candidate shapes on `syndromes` (device tensor) with ``decode_fn`` (default
-    ``dec.decode``); configure and return the fastest (median of ``repeats`` runs)."""
+    ``dec.decode``); configure and return the fastest (median of ``repeats`` runs).  ``kind``
+    "pre" or "legs" tunes only that launch kind's shape, the other kind keeping its own."""
     B = int(syndromes.shape[0])
-    key = cache_key(dec, B) + ("" if decode_fn is None else "|custom")
-    if use_cache and decode_fn is None:
+    key = cache_key(dec, B) + ("" if decode_fn is None else "|custom") + ("" if kind == "all" else f"|{kind}")
+    if use_cache and decode_fn is None and kind == "all":
         hit = lookup(dec, B)
         if hit is not None:
             dec.configure_launch(*hit)
@@ -137,19 +168,22 @@ def tune(dec, syndromes: torch.Tensor, shapes: Optional[Iterable[Tuple[int, ...]
     shapes = list(shapes) if shapes is not None else candidates(dec.C, dec.V)
     for shape in shapes:
         try:
-            dec.configure_launch(*shape)
+            dec.configure_launch(*shape, kind=kind)
         except (NotImplementedError, ValueError):
             continue
         ms = _time(lambda: fn(syndromes), repeats)
         info = dec.launch_info()
-        got = (info["group_threads"], info["groups_per_block"], info["shots_per_group"])
+        if kind == "pre":
+            info = info["pre"]
+        got = (info["group_threads"], info["groups_per_block"], info["shots_per_group"], info["blocks_per_sm"])
         results.append((ms, got))
         if verbose:
-            print(f"  G={got[0]:4d} groups={got[1]:2d} shots/group={got[2]}: {ms:8.3f} ms", flush=True)
+            print(f"  G={got[0]:4d} groups={got[1]:2d} shots/group={got[2]} blocks/SM={got[3]}: {ms:8.3f} ms",
+                  flush=True)
     if not results:
         raise RuntimeError("no launch shape could be configured")
     ms, shape = min(results)
-    dec.configure_launch(*shape)
+    dec.configure_launch(*shape, kind=kind)
     _store(key, {"shape": list(shape), "ms": ms, "sample_shots": B,
                  "tried": [[list(s), t] for t, s in sorted(results)]})
     return shape

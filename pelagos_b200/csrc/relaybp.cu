@@ -47,12 +47,16 @@ struct rbp_decoder {
   DevBuf<float> alpha;
   DevBuf<int> queue;
   int n_alpha = 0;
-  // launch shape
-  KernelFn kernel = nullptr;
-  int group_threads = 0, groups = 0, blocks = 0, vpt = 0;
-  int nshots = 1;              // shots a group decodes at once
-  int slots_kernel = 0;        // 1: relaybp_slots_kernel (one group per block)
-  int group_bytes = 0, block_bytes = 0;
+  // launch shapes: shape[0] for launches that skip the relay legs (pre-iterations
+  // only, so a shot's latency is bounded by pre_iter), shape[1] for the others
+  struct Shape {
+    KernelFn kernel = nullptr;
+    int group_threads = 0, groups = 0, blocks = 0, vpt = 0;
+    int nshots = 1;            // shots a group decodes at once
+    int slots_kernel = 0;      // 1: relaybp_slots_kernel (one group per block)
+    int minb = 1;              // resident blocks per SM the kernel is compiled for
+    int group_bytes = 0, block_bytes = 0;
+  } shape[2];
   int sm_count = 0;
   size_t max_smem = 0;
 };
@@ -121,12 +125,12 @@ KernelFn pick_kernel(int msg_type, int dc, int dv, int vpt) {
   }
 }
 
-KernelFn pick_slots_kernel(int msg_type, int dc, int dv, int vpt, int ns) {
+KernelFn pick_slots_kernel(int msg_type, int dc, int dv, int vpt, int ns, int minb) {
   switch (msg_type) {
-    case RBP_MSG_F32: return rbpk::pick_slots_f32(dc, dv, vpt, ns);
-    case RBP_MSG_F16: return rbpk::pick_slots_f16(dc, dv, vpt, ns);
-    case RBP_MSG_BF16: return rbpk::pick_slots_bf16(dc, dv, vpt, ns);
-    case RBP_MSG_F64: return rbpk::pick_slots_f64(dc, dv, vpt, ns);
+    case RBP_MSG_F32: return rbpk::pick_slots_f32(dc, dv, vpt, ns, minb);
+    case RBP_MSG_F16: return rbpk::pick_slots_f16(dc, dv, vpt, ns, minb);
+    case RBP_MSG_BF16: return rbpk::pick_slots_bf16(dc, dv, vpt, ns, minb);
+    case RBP_MSG_F64: return rbpk::pick_slots_f64(dc, dv, vpt, ns, minb);
     default: return nullptr;
   }
 }
@@ -141,11 +145,12 @@ int vpt_for(int V, int G) {
 
 // Default shape: the fewest owned variables per thread (from 3 up) whose group
 // still fits the register budget of that count (of the one- or two-shot
-// kernel), so a shot's iteration is short.
-int default_group_threads(int C, int V, int nshots = 1, int vslots = 8) {
+// kernel, at one or two resident blocks per SM), so a shot's iteration is short.
+int default_group_threads(int C, int V, int nshots = 1, int vslots = 8, int minb = 1) {
   for (int vpt : {3, 4, 6, 8, 12, 16}) {
     const int G = std::max(32, (V + vpt - 1) / vpt + 31) / 32 * 32;
-    const int max_threads = rbpk::max_slots_block_threads(vpt, nshots, vslots <= 3 ? 3 : 8);
+    const int max_threads = minb == 2 ? rbpk::max_slots_block_threads2(vpt)
+                                      : rbpk::max_slots_block_threads(vpt, nshots, vslots <= 3 ? 3 : 8);
     if (G <= max_threads && (C + G - 1) / G <= 32 && vpt_for(V, G) <= vpt) return G;
   }
   return 256;  // configure reports why no shape fits
@@ -169,22 +174,27 @@ struct Launch {
   int group_threads, groups, blocks;
   int nshots;        // shots a group decodes at once
   int slots_kernel;  // 1: relaybp_slots_kernel (one group per block, nshots shot regions)
+  int minb;          // resident blocks per SM the kernel is compiled for
 };
 
 // Block-per-group shape: one group of G threads per block with nshots shot regions
-// (relaybp_slots_kernel).
-int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int nshots,
+// (relaybp_slots_kernel), compiled for minb (1 or 2) resident blocks per SM.
+int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int nshots, int minb,
                         size_t max_smem, int sm_count, Launch* out, const std::string& w) {
   const int vpt = vpt_for(V, G);
-  const int max_threads = rbpk::max_slots_block_threads(vpt, nshots, vslots <= 3 ? 3 : 8);
+  const int max_threads = minb == 2 ? rbpk::max_slots_block_threads2(vpt)
+                                    : rbpk::max_slots_block_threads(vpt, nshots, vslots <= 3 ? 3 : 8);
   if (G > max_threads)
     return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(G) + " threads with " + std::to_string(vpt) +
                                          " variables each exceed the register budget of " + std::to_string(nshots) +
-                                         "-shot groups");
-  KernelFn k = pick_slots_kernel(msg_type, slots, vslots, vpt, nshots);
+                                         "-shot groups" + (minb == 2 ? " at two blocks per SM" : ""));
+  KernelFn k = pick_slots_kernel(msg_type, slots, vslots, vpt, nshots, minb);
   if (!k)
-    return fail(RBP_ERR_UNSUPPORTED, w + ": no block-per-group kernel for this degree / shape (check degrees "
-                                         "above 16 run with several groups per block, one shot each)");
+    return fail(RBP_ERR_UNSUPPORTED,
+                w + (minb == 2 ? ": no two-blocks-per-SM kernel for this shape (one shot per group, check "
+                                 "degrees up to 16)"
+                               : ": no block-per-group kernel for this degree / shape (check degrees "
+                                 "above 16 run with several groups per block, one shot each)"));
   const Layout L = make_layout(C, V, rows, msg_type, G);
   const size_t smem = (size_t)L.off_group0 + (size_t)nshots * L.group_bytes;
   if (smem > max_smem)
@@ -194,14 +204,16 @@ int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_t
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G, smem));
   if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
-  *out = Launch{k, G, 1, per_sm * sm_count, nshots, 1};
+  *out = Launch{k, G, 1, per_sm * sm_count, nshots, 1, minb};
   return RBP_OK;
 }
 
 // Kernel and launch shape for G threads per group (groups_per_block 0: as many
-// as fit) decoding `nshots` shots at once (1 or 2).
+// as fit) decoding `nshots` shots at once (1 or 2); blocks_per_sm 2 selects the
+// block-per-group kernel compiled for two resident blocks per SM.
 int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, int G, int groups_per_block,
-                  size_t max_smem, int sm_count, Launch* out, const char* who, int nshots = 1) {
+                  size_t max_smem, int sm_count, Launch* out, const char* who, int nshots = 1,
+                  int blocks_per_sm = 1) {
   const std::string w(who);
   if (G % 32 != 0 || G > 1024)
     return fail(RBP_ERR_ARGUMENT, w + ": group_threads must be a multiple of 32, at most 1024");
@@ -209,11 +221,17 @@ int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, i
   const int vpt = vpt_for(V, G);
   if (vpt < 0) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 16 variables per thread; use more group threads");
   if ((C + G - 1) / G > 32) return fail(RBP_ERR_UNSUPPORTED, w + ": more than 32 checks per thread; use more group threads");
+  if (blocks_per_sm != 1 && blocks_per_sm != 2)
+    return fail(RBP_ERR_ARGUMENT, w + ": blocks_per_sm must be 0 (one), 1 or 2");
+  if (blocks_per_sm == 2 && (nshots != 1 || groups_per_block != 1))
+    return fail(RBP_ERR_UNSUPPORTED, w + ": two blocks per SM run the block-per-group kernel with one shot per "
+                                         "group (groups_per_block 1, shots_per_group 1)");
   // groups_per_block 1, or two shots per group: the block-per-group kernel
   if (nshots == 2 || groups_per_block == 1) {
     if (groups_per_block > 1)
       return fail(RBP_ERR_UNSUPPORTED, w + ": two-shot groups run one group per block");
-    return choose_slots_launch(C, V, slots, vslots, rows, msg_type, G, nshots, max_smem, sm_count, out, w);
+    return choose_slots_launch(C, V, slots, vslots, rows, msg_type, G, nshots, blocks_per_sm, max_smem, sm_count,
+                               out, w);
   }
   const int max_threads = rbpk::max_block_threads(vpt);
   if (G > max_threads)
@@ -238,7 +256,7 @@ int choose_launch(int C, int V, int slots, int vslots, int rows, int msg_type, i
   int per_sm = 0;
   RBP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G * NG, smem));
   if (per_sm < 1) return fail(RBP_ERR_UNSUPPORTED, w + ": launch shape has zero occupancy");
-  *out = Launch{k, G, NG, per_sm * sm_count, 1, 0};
+  *out = Launch{k, G, NG, per_sm * sm_count, 1, 0, 1};
   return RBP_OK;
 }
 
@@ -449,7 +467,17 @@ int rbp_graph_destroy(rbp_graph* g) {
 
 int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_per_block,
                           int32_t shots_per_group) {
+  return rbp_decoder_configure_kind(d, RBP_LAUNCH_ALL, group_threads, groups_per_block, shots_per_group, 0);
+}
+
+int rbp_decoder_configure_kind(rbp_decoder* d, int32_t kind, int32_t group_threads, int32_t groups_per_block,
+                               int32_t shots_per_group, int32_t blocks_per_sm) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: null decoder");
+  if (kind < RBP_LAUNCH_ALL || kind > RBP_LAUNCH_LEGS)
+    return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: kind must be RBP_LAUNCH_ALL, _PRE or _LEGS");
+  if (blocks_per_sm < 0 || blocks_per_sm > 2)
+    return fail(RBP_ERR_ARGUMENT, "rbp_decoder_configure: blocks_per_sm must be 0 (one), 1 or 2");
+  const int minb = blocks_per_sm == 2 ? 2 : 1;
   const rbp_graph* g = d->g;
   const int nshots = shots_per_group > 0 ? shots_per_group : 1;
   // groups_per_block 0 (default) or -1: the multi-group kernel with as many one-shot groups
@@ -461,22 +489,26 @@ int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t groups_
   const bool block_per_group = nshots == 2 || groups_per_block == 1;
   // default group size within the register budget of the kernel family that runs it
   const int G = group_threads > 0 ? group_threads
-                                  : default_group_threads(g->C, g->V, nshots, block_per_group ? g->vslots : 8);
+                                  : default_group_threads(g->C, g->V, nshots, block_per_group ? g->vslots : 8, minb);
   DeviceGuard dg(g->device);
   Launch lc{};
   const int rc = choose_launch(g->C, g->V, g->slots, g->vslots, d->rows, d->p.msg_type, G, groups_per_block,
-                               d->max_smem, d->sm_count, &lc, "rbp_decoder_configure", nshots);
+                               d->max_smem, d->sm_count, &lc, "rbp_decoder_configure", nshots, minb);
   if (rc != RBP_OK) return rc;
   const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, G);
-  d->kernel = lc.kernel;
-  d->vpt = vpt_for(g->V, G);
-  d->group_threads = lc.group_threads;
-  d->groups = lc.groups;
-  d->blocks = lc.blocks;
-  d->nshots = lc.nshots;
-  d->slots_kernel = lc.slots_kernel;
-  d->group_bytes = L.group_bytes;
-  d->block_bytes = L.off_group0;
+  rbp_decoder::Shape sh;
+  sh.kernel = lc.kernel;
+  sh.vpt = vpt_for(g->V, G);
+  sh.group_threads = lc.group_threads;
+  sh.groups = lc.groups;
+  sh.blocks = lc.blocks;
+  sh.nshots = lc.nshots;
+  sh.slots_kernel = lc.slots_kernel;
+  sh.minb = lc.minb;
+  sh.group_bytes = L.group_bytes;
+  sh.block_bytes = L.off_group0;
+  if (kind != RBP_LAUNCH_LEGS) d->shape[0] = sh;
+  if (kind != RBP_LAUNCH_PRE) d->shape[1] = sh;
   return RBP_OK;
 }
 
@@ -569,12 +601,23 @@ int rbp_state_posterior_offset(const rbp_decoder* d, int64_t* offset) {
 int rbp_decoder_query(const rbp_decoder* d, int64_t* group_smem, int64_t* block_smem, int32_t* group_threads,
                       int32_t* groups_per_block, int32_t* blocks, int32_t* shots_per_group) {
   if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_query: null decoder");
-  if (shots_per_group) *shots_per_group = d->nshots;
-  if (group_smem) *group_smem = d->group_bytes;
-  if (block_smem) *block_smem = d->block_bytes;
-  if (group_threads) *group_threads = d->group_threads;
-  if (groups_per_block) *groups_per_block = d->groups;
-  if (blocks) *blocks = d->blocks;
+  if (group_smem) *group_smem = d->shape[1].group_bytes;
+  if (block_smem) *block_smem = d->shape[1].block_bytes;
+  return rbp_decoder_query_kind(d, RBP_LAUNCH_LEGS, group_threads, groups_per_block, shots_per_group, nullptr,
+                                blocks);
+}
+
+int rbp_decoder_query_kind(const rbp_decoder* d, int32_t kind, int32_t* group_threads, int32_t* groups_per_block,
+                           int32_t* shots_per_group, int32_t* blocks_per_sm, int32_t* blocks) {
+  if (!d) return fail(RBP_ERR_ARGUMENT, "rbp_decoder_query: null decoder");
+  if (kind != RBP_LAUNCH_PRE && kind != RBP_LAUNCH_LEGS)
+    return fail(RBP_ERR_ARGUMENT, "rbp_decoder_query: kind must be RBP_LAUNCH_PRE or RBP_LAUNCH_LEGS");
+  const rbp_decoder::Shape& sh = d->shape[kind == RBP_LAUNCH_PRE ? 0 : 1];
+  if (group_threads) *group_threads = sh.group_threads;
+  if (groups_per_block) *groups_per_block = sh.groups;
+  if (shots_per_group) *shots_per_group = sh.nshots;
+  if (blocks_per_sm) *blocks_per_sm = sh.minb;
+  if (blocks) *blocks = sh.blocks;
   return RBP_OK;
 }
 
@@ -585,9 +628,11 @@ int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs
   const rbp_graph* g = d->g;
   DeviceGuard dg(g->device);
   if (!dg.ok) return fail(RBP_ERR_CUDA, "rbp_decode: cannot select the CUDA device");
-  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, d->group_threads);
+  // a launch that skips the relay legs runs at most pre_iter iterations per shot
+  const rbp_decoder::Shape& sh = d->shape[in->skip_relay_legs ? 0 : 1];
+  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, sh.group_threads);
   const DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
-  const Launch lc{d->kernel, d->group_threads, d->groups, d->blocks, d->nshots, d->slots_kernel};
+  const Launch lc{sh.kernel, sh.group_threads, sh.groups, sh.blocks, sh.nshots, sh.slots_kernel, sh.minb};
   return launch_decode(dgph, d->p, L, lc, d->llr.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
                        out, reinterpret_cast<cudaStream_t>(stream), "rbp_decode");
 }
@@ -728,7 +773,7 @@ int rbp_mixed_create(const rbp_decoder* const* decoders, int32_t n, rbp_mixed** 
       return fail(RBP_ERR_ARGUMENT, "rbp_mixed_create: all decoders must be on one device");
     dc = std::max(dc, d->g->slots);
     dv = std::max(dv, d->g->vslots);
-    vpt_need = std::max(vpt_need, vpt_for(d->g->V, std::min(d->group_threads, 512)));
+    vpt_need = std::max(vpt_need, vpt_for(d->g->V, std::min(d->shape[1].group_threads, 512)));
   }
   // The vectorised check pass moves MAXDC slots per row (8 or 16), so every
   // code's padded layout must have exactly that many rows; codes whose rows

@@ -59,6 +59,15 @@ __host__ __device__ constexpr int max_slots_block_threads(int vpt, int ns = 2, i
                  : (vpt <= 4 ? 512 : (vpt == 6 ? 480 : (vpt == 8 ? 384 : (vpt == 12 ? 256 : 192))));
 }
 
+// Largest block of the one-shot instantiations compiled for two resident
+// blocks per SM (MINB 2): each block gets half the register file, so the
+// owned-variable state is capped at 64 registers (VPT <= 6) or 80 (VPT 8).
+// Two shots then decode side by side on one SM with their own barriers, so
+// one block's barrier and dependency waits are filled by the other's work.
+__host__ __device__ constexpr int max_slots_block_threads2(int vpt) {
+  return vpt <= 4 ? 512 : (vpt == 6 ? 480 : (vpt == 8 ? 384 : 256));
+}
+
 template <typename A, int VPT>
 struct SlotState {
   A post[VPT];          // posteriors of the owned variables (the memory)
@@ -879,10 +888,13 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   }
 }
 
-// One code, one group of NS shots per block (rbp_decode with groups_per_block 1).
-template <typename M, int MAXDC, int VPT, int MAXDV, int NS>
-__global__ void __launch_bounds__(max_slots_block_threads(VPT, NS, MAXDV), 1)
+// One code, one group of NS shots per block (rbp_decode with groups_per_block 1),
+// compiled for MINB resident blocks per SM (1, or 2 for one-shot groups).
+template <typename M, int MAXDC, int VPT, int MAXDV, int NS, int MINB>
+__global__ void __launch_bounds__(MINB == 2 ? max_slots_block_threads2(VPT) : max_slots_block_threads(VPT, NS, MAXDV),
+                                  MINB)
 relaybp_slots_kernel(DevGraph g, DevArgs a) {
+  static_assert(MINB == 1 || (MINB == 2 && NS == 1), "two resident blocks per SM: one-shot groups only");
   extern __shared__ __align__(16) unsigned char smem[];
   load_block_tables(g, a, smem);
   __syncthreads();
@@ -891,38 +903,56 @@ relaybp_slots_kernel(DevGraph g, DevArgs a) {
 }
 
 // Kernel for (check degree bound, variable degree, owned variables per thread,
-// shots per group 1 or 2), or null when this build has no such instantiation.
-KernelFn pick_slots_f32(int dc, int dv, int vpt, int ns);
-KernelFn pick_slots_f16(int dc, int dv, int vpt, int ns);
-KernelFn pick_slots_bf16(int dc, int dv, int vpt, int ns);
-KernelFn pick_slots_f64(int dc, int dv, int vpt, int ns);
+// shots per group 1 or 2, resident blocks per SM 1 or 2), or null when this
+// build has no such instantiation (two blocks per SM: one shot per group).
+KernelFn pick_slots_f32(int dc, int dv, int vpt, int ns, int minb);
+KernelFn pick_slots_f16(int dc, int dv, int vpt, int ns, int minb);
+KernelFn pick_slots_bf16(int dc, int dv, int vpt, int ns, int minb);
+KernelFn pick_slots_f64(int dc, int dv, int vpt, int ns, int minb);
 
 }  // namespace rbpk
 
 // Instantiation table of the block-per-group kernel for one message type
 // (check rows of at most 8 or 16 slots; wider rows use relaybp_decode_kernel).
-#define RBPK_SLOTS_DC_DV(M, DC, VPT, NS)                                       \
-  if (dv <= 3) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 3, NS>;          \
-  if (dv <= 8) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 8, NS>;          \
+#define RBPK_SLOTS_DC_DV(M, DC, VPT, NS, MB)                                   \
+  if (dv <= 3) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 3, NS, MB>;      \
+  if (dv <= 8) return &rbpk::relaybp_slots_kernel<M, DC, VPT, 8, NS, MB>;      \
   return nullptr;
-#define RBPK_SLOTS_DC(M, VPT, NS)                                              \
-  if (dc <= 8) { RBPK_SLOTS_DC_DV(M, 8, VPT, NS) }                             \
-  if (dc <= 16) { RBPK_SLOTS_DC_DV(M, 16, VPT, NS) }                           \
+#define RBPK_SLOTS_DC(M, VPT, NS, MB)                                          \
+  if (dc <= 8) { RBPK_SLOTS_DC_DV(M, 8, VPT, NS, MB) }                         \
+  if (dc <= 16) { RBPK_SLOTS_DC_DV(M, 16, VPT, NS, MB) }                       \
   return nullptr;
 #define RBPK_SLOTS_VPT(M, NS)                                                  \
   switch (vpt) {                                                               \
-    case 1: { RBPK_SLOTS_DC(M, 1, NS) }                                        \
-    case 2: { RBPK_SLOTS_DC(M, 2, NS) }                                        \
-    case 3: { RBPK_SLOTS_DC(M, 3, NS) }                                        \
-    case 4: { RBPK_SLOTS_DC(M, 4, NS) }                                        \
-    case 6: { RBPK_SLOTS_DC(M, 6, NS) }                                        \
-    case 8: { RBPK_SLOTS_DC(M, 8, NS) }                                        \
-    case 12: { RBPK_SLOTS_DC(M, 12, NS) }                                      \
-    case 16: { RBPK_SLOTS_DC(M, 16, NS) }                                      \
+    case 1: { RBPK_SLOTS_DC(M, 1, NS, 1) }                                     \
+    case 2: { RBPK_SLOTS_DC(M, 2, NS, 1) }                                     \
+    case 3: { RBPK_SLOTS_DC(M, 3, NS, 1) }                                     \
+    case 4: { RBPK_SLOTS_DC(M, 4, NS, 1) }                                     \
+    case 6: { RBPK_SLOTS_DC(M, 6, NS, 1) }                                     \
+    case 8: { RBPK_SLOTS_DC(M, 8, NS, 1) }                                     \
+    case 12: { RBPK_SLOTS_DC(M, 12, NS, 1) }                                   \
+    case 16: { RBPK_SLOTS_DC(M, 16, NS, 1) }                                   \
     default: return nullptr;                                                   \
   }
+#define RBPK_SLOTS_VPT_2PERSM(M)                                               \
+  switch (vpt) {                                                               \
+    case 1: { RBPK_SLOTS_DC(M, 1, 1, 2) }                                      \
+    case 2: { RBPK_SLOTS_DC(M, 2, 1, 2) }                                      \
+    case 3: { RBPK_SLOTS_DC(M, 3, 1, 2) }                                      \
+    case 4: { RBPK_SLOTS_DC(M, 4, 1, 2) }                                      \
+    case 6: { RBPK_SLOTS_DC(M, 6, 1, 2) }                                      \
+    case 8: { RBPK_SLOTS_DC(M, 8, 1, 2) }                                      \
+    case 12: { RBPK_SLOTS_DC(M, 12, 1, 2) }                                    \
+    case 16: { RBPK_SLOTS_DC(M, 16, 1, 2) }                                    \
+    default: return nullptr;                                                   \
+  }
+
 #define RBPK_DEFINE_PICK_SLOTS(NAME, M)                                        \
-  rbpk::KernelFn rbpk::NAME(int dc, int dv, int vpt, int ns) {                 \
+  rbpk::KernelFn rbpk::NAME(int dc, int dv, int vpt, int ns, int minb) {       \
+    if (minb == 2) {                                                           \
+      if (ns == 1) { RBPK_SLOTS_VPT_2PERSM(M) }                                \
+      return nullptr;                                                          \
+    }                                                                          \
     if (ns == 1) { RBPK_SLOTS_VPT(M, 1) }                                      \
     if (ns == 2) { RBPK_SLOTS_VPT(M, 2) }                                      \
     return nullptr;                                                            \

@@ -98,17 +98,29 @@ class _NativeDecoder:
         llr = np.ascontiguousarray(llr, dtype=np.float32)
         nat.check(nat.lib().rbp_decoder_set_llr(self._dec, nat.f32_ptr(llr)), "rbp_decoder_set_llr")
 
-    def configure(self, group_threads: int, groups_per_block: int, shots_per_group: int = 0):
-        nat.check(nat.lib().rbp_decoder_configure(self._dec, int(group_threads), int(groups_per_block),
-                                                  int(shots_per_group)), "rbp_decoder_configure")
+    def configure(self, group_threads: int, groups_per_block: int, shots_per_group: int = 0,
+                  blocks_per_sm: int = 0, kind: int = nat.RBP_LAUNCH_ALL):
+        nat.check(nat.lib().rbp_decoder_configure_kind(self._dec, int(kind), int(group_threads),
+                                                       int(groups_per_block), int(shots_per_group),
+                                                       int(blocks_per_sm)), "rbp_decoder_configure")
 
     def query(self) -> dict:
         gs, bs = ct.c_int64(), ct.c_int64()
         gt, gb, nb, ns = ct.c_int32(), ct.c_int32(), ct.c_int32(), ct.c_int32()
         nat.check(nat.lib().rbp_decoder_query(self._dec, ct.byref(gs), ct.byref(bs), ct.byref(gt),
                                               ct.byref(gb), ct.byref(nb), ct.byref(ns)), "rbp_decoder_query")
-        return {"group_smem": gs.value, "block_smem": bs.value, "group_threads": gt.value,
-                "groups_per_block": gb.value, "blocks": nb.value, "shots_per_group": ns.value}
+        out = {"group_smem": gs.value, "block_smem": bs.value, "group_threads": gt.value,
+               "groups_per_block": gb.value, "blocks": nb.value, "shots_per_group": ns.value}
+        for kind, key in ((nat.RBP_LAUNCH_LEGS, None), (nat.RBP_LAUNCH_PRE, "pre")):
+            gt, gb, ns, bps, nb = (ct.c_int32() for _ in range(5))
+            nat.check(nat.lib().rbp_decoder_query_kind(self._dec, kind, ct.byref(gt), ct.byref(gb), ct.byref(ns),
+                                                       ct.byref(bps), ct.byref(nb)), "rbp_decoder_query")
+            if key is None:
+                out["blocks_per_sm"] = bps.value
+            else:
+                out[key] = {"group_threads": gt.value, "groups_per_block": gb.value, "shots_per_group": ns.value,
+                            "blocks_per_sm": bps.value, "blocks": nb.value}
+        return out
 
     def decode(self, B: int, batch: nat.RbpBatch, outs: nat.RbpOutputs, stream: int):
         nat.check(nat.lib().rbp_decode(self._dec, int(B), ct.byref(batch), ct.byref(outs),
@@ -137,8 +149,10 @@ class RelayBPDecoder:
 
     * ``mix_rounding``: rounding of the memory mix (1-g)*llr + g*posterior:
       "separate" (default; one rounding per operation), "fma_gp" or "fma_lp";
-    * ``launch``: optional (group_threads, groups_per_block[, shots_per_group]) kernel shape;
-      shots_per_group 2 selects the kernel whose groups decode two shots at once.
+    * ``launch``: optional (group_threads, groups_per_block[, shots_per_group[, blocks_per_sm]])
+      kernel shape of every launch; shots_per_group 2 selects the kernel whose groups decode two
+      shots at once, blocks_per_sm 2 the one-shot kernel compiled for two resident blocks per SM.
+      ``configure_launch(..., kind="pre")`` gives the pre-iteration launches their own shape.
     * ``hard_shots_first`` (default True): a relay decode of at least 1024 shots
       runs as two launches, the pre-iterations and then the relay legs resumed
       from each shot's saved state, with the shots the pre-iterations left
@@ -285,6 +299,7 @@ class RelayBPDecoder:
         torch.manual_seed(seed)
 
         self._launch = tuple(launch) if launch is not None else None
+        self._pre_launch = None  # shape of the pre-iteration launches when it differs from _launch
         self.hard_shots_first = bool(hard_shots_first)
         if parity_first not in (0, 1, 2):
             raise ValueError("parity_first must be 0, 1 or 2")
@@ -374,16 +389,32 @@ class RelayBPDecoder:
                                 self._leg_table(gpu_id), alpha)
             if self._launch is not None:
                 nd.configure(*self._launch)
+            if self._pre_launch is not None:
+                nd.configure(*self._pre_launch, kind=nat.RBP_LAUNCH_PRE)
         return nd
 
     # ------------------------------------------------------------------ public helpers
 
-    def configure_launch(self, group_threads: int, groups_per_block: int, shots_per_group: int = 0) -> None:
+    def configure_launch(self, group_threads: int, groups_per_block: int, shots_per_group: int = 0,
+                         blocks_per_sm: int = 0, kind: str = "all") -> None:
         """Set the kernel shape (threads per shot group, groups per thread block, shots a group
-        decodes at once; 0 picks the default)."""
-        self._launch = (int(group_threads), int(groups_per_block), int(shots_per_group))
+        decodes at once, resident blocks per SM the kernel is compiled for; 0 picks the default)
+        of every launch (``kind="all"``), of the launches that run only the pre-iterations
+        (``"pre"``: the first launch of a two-launch decode), or of the others (``"legs"``)."""
+        if kind not in ("all", "pre", "legs"):
+            raise ValueError("kind must be 'all', 'pre' or 'legs'")
+        shape = (int(group_threads), int(groups_per_block), int(shots_per_group), int(blocks_per_sm))
+        code = {"all": nat.RBP_LAUNCH_ALL, "pre": nat.RBP_LAUNCH_PRE, "legs": nat.RBP_LAUNCH_LEGS}[kind]
         for nd in self._native.values():
-            nd.configure(*self._launch)
+            nd.configure(*shape, kind=code)
+        if kind == "all":
+            self._launch, self._pre_launch = shape, None
+        elif kind == "pre":
+            self._pre_launch = shape
+        else:
+            if self._pre_launch is None:  # the pre-iteration launches keep their current shape
+                self._pre_launch = self._launch if self._launch is not None else (0, 0, 0, 0)
+            self._launch = shape
 
     def launch_info(self) -> dict:
         return self._native[self.device_ids[0]].query()

@@ -310,7 +310,10 @@ class LearnedRelayBPDecoder:
         """(graph, static input, buffers) of this batch size and buffer set; captured on first
         use from an eager warm-up decode of ``syn``."""
         B = int(syn.shape[0])
+        shapes = (self.dec._launch, self.dec._pre_launch)  # a graph keeps the kernel shapes it captured
         entry = self._graphs.get((B, slot))
+        if entry is not None and entry[3] != shapes:
+            entry = None
         if entry is None:
             static = torch.empty(B, self.dec.C, dtype=torch.uint8, device=self.net.device)
             static.copy_(syn)
@@ -319,13 +322,13 @@ class LearnedRelayBPDecoder:
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
                 bf = self.decode_into(static, slot=slot)
-            entry = (g, static, bf)
+            entry = (g, static, bf, shapes)
             self._graphs[(B, slot)] = entry
         return entry
 
     def _replay(self, syn: torch.Tensor) -> dict:
         """Copy the syndromes (host or device) into the captured input buffer and replay."""
-        g, static, bf = self._graph_entry(syn)
+        g, static, bf, _ = self._graph_entry(syn)
         static.copy_(syn, non_blocking=True)
         g.replay()
         return bf
@@ -495,7 +498,7 @@ class LearnedRelayBPDecoder:
 
         bring_in(0)
         for i in range(n):
-            g, _, bf = entries[i % 2]
+            g, _, bf, _ = entries[i % 2]
             compute.wait_event(h2d[i])
             g.replay()
             decoded = torch.cuda.Event()

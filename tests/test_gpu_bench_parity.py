@@ -6,8 +6,9 @@ phenomenological workload at p = 0.003 (seed 2026), full Relay-BP-S schedule
 decoded on the GPU and compared bit for bit with the CPU oracle:
 
 * the plain decoder (RelayBPDecoder.decode), with every kernel family (the
-  block-per-group kernel with one and with two shots per group, and the kernel
-  whose blocks hold several one-shot groups);
+  block-per-group kernel with one and with two shots per group, the kernel
+  whose blocks hold several one-shot groups, and the benchmark's committed
+  shape: 352-thread one-shot groups at two resident blocks per SM);
 * the gated learned decoder (LearnedRelayBPDecoder, gate=True) against the
   oracle's per-shot emulation of it: shots the pre-iterations solved run relay
   legs 0-3 at the constant top strength, the others run them with the
@@ -74,23 +75,23 @@ def plain_oracle(bench_batch):
     return _oracle_chunks(dec, syn, dec._leg_table(0))
 
 
-@pytest.mark.parametrize("nshots", [(1, 1), (1, 2), (0, 1)])
-def test_plain_decode_of_the_bench_batch_matches_oracle(bench_batch, plain_oracle, nshots):
+@pytest.mark.parametrize("launch", [(0, 1, 1), (0, 1, 2), (0, 0, 1), (352, 1, 1, 2)])
+def test_plain_decode_of_the_bench_batch_matches_oracle(bench_batch, plain_oracle, launch):
     w, syn = bench_batch
-    dec = RelayBPDecoder(w.H, w.priors, launch=(0, *nshots), **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, launch=launch, **RELAY)
     out = dec.decode(torch.from_numpy(syn).to(DEV))
     got = {k: out[k].cpu().numpy() for k in KEYS}
-    _assert_same(got, plain_oracle, f"plain decode, launch {nshots}")
+    _assert_same(got, plain_oracle, f"plain decode, launch {launch}")
     # the long relay tails are exercised
     assert got["iterations"].max() > 200
 
 
-@pytest.mark.parametrize("nshots", [(1, 1), (1, 2), (0, 1)])
-def test_gated_learned_decode_of_the_bench_batch_matches_oracle_emulation(bench_batch, nshots):
+@pytest.mark.parametrize("launch", [(0, 1, 1), (0, 1, 2), (0, 0, 1), (352, 1, 1, 2)])
+def test_gated_learned_decode_of_the_bench_batch_matches_oracle_emulation(bench_batch, launch):
     from pelagos_b200.proposal import LearnedRelayBPDecoder, ProposalNet, default_weights_path, load_params
 
     w, syn = bench_batch
-    dec = RelayBPDecoder(w.H, w.priors, launch=(0, *nshots), **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, launch=launch, **RELAY)
     net = ProposalNet(dec, load_params(default_weights_path("bb144_phen", P))[0])
     learned = LearnedRelayBPDecoder(dec, net, learned_legs=4, gate=True, graph=False)
     syn_d = torch.from_numpy(syn).to(DEV)
@@ -114,4 +115,4 @@ def test_gated_learned_decode_of_the_bench_batch_matches_oracle_emulation(bench_
     for k in KEYS:
         want[k][sol] = r_sol[k]
         want[k][uns] = r_uns[k]
-    _assert_same(got, want, f"gated learned decode, launch {nshots}")
+    _assert_same(got, want, f"gated learned decode, launch {launch}")

@@ -54,7 +54,7 @@ def _golden_decode_kwargs(g):
 
 #: kernel families, as (groups_per_block, shots_per_group): the block-per-group kernel with one
 #: and with two shots per group, and the (default) kernel whose blocks hold several one-shot groups
-NSHOTS = [(1, 1), (1, 2), (0, 1)]
+NSHOTS = [(1, 1), (1, 2), (0, 1), (1, 1, 2)]  # block-per-group (one, two shots), multi-group, two blocks per SM
 
 
 @pytest.mark.parametrize("nshots", NSHOTS)
@@ -247,7 +247,8 @@ def test_full_size_batch_and_permutation_invariance(bb144_full):
 
 
 @pytest.mark.parametrize("shape", [(192, 1), (256, 1), (448, 1), (512, 1), (768, 1), (864, 1),
-                                   (256, 1, 2), (384, 1, 2), (448, 1, 2), (480, 1, 2)])
+                                   (256, 1, 2), (384, 1, 2), (448, 1, 2), (480, 1, 2),
+                                   (256, 1, 1, 2), (352, 1, 1, 2), (448, 1, 1, 2), (480, 1, 1, 2)])
 def test_launch_shape_invariance(shape):
     w = codes.workload("bb144_phen")
     err, syn = w.sample(512, seed=12)
@@ -257,3 +258,36 @@ def test_launch_shape_invariance(shape):
     oa, ob = _np(a.decode(s)), _np(b.decode(s))
     for k in KEYS:
         np.testing.assert_array_equal(oa[k], ob[k])
+
+
+@pytest.mark.parametrize("pre,legs", [((352, 1, 1, 2), (704, 1, 1)), ((704, 1, 1), (352, 1, 1, 2)),
+                                      ((448, 1, 1, 2), (480, 1, 1, 2))])
+def test_per_kind_launch_shapes(pre, legs):
+    """The pre-iteration launch and the relay-leg launch of a two-launch decode take their own
+    shapes (reported by launch_info) and give the single-shape result."""
+    w = codes.workload("bb144_phen")
+    err, syn = w.sample(2048, seed=21)
+    a = RelayBPDecoder(w.H, w.priors, **RELAY)
+    b = RelayBPDecoder(w.H, w.priors, **RELAY)
+    b.configure_launch(*legs, kind="legs")
+    b.configure_launch(*pre, kind="pre")
+    info = b.launch_info()
+    assert (info["group_threads"], info["blocks_per_sm"]) == (legs[0], legs[3] if len(legs) > 3 else 1)
+    assert (info["pre"]["group_threads"], info["pre"]["blocks_per_sm"]) == (pre[0], pre[3] if len(pre) > 3 else 1)
+    for shape, i in ((pre, info["pre"]), (legs, info)):
+        assert i["blocks"] == (2 if len(shape) > 3 else 1) * torch.cuda.get_device_properties(0).multi_processor_count
+    s = torch.from_numpy(syn).to(DEV)
+    oa, ob = _np(a.decode(s)), _np(b.decode(s))
+    for k in KEYS:
+        np.testing.assert_array_equal(oa[k], ob[k])
+
+
+def test_two_blocks_per_sm_rejects_shapes_outside_its_budget():
+    w = codes.workload("bb144_phen")
+    dec = RelayBPDecoder(w.H, w.priors, **RELAY)
+    with pytest.raises(NotImplementedError, match="register budget"):
+        dec.configure_launch(704, 1, 1, 2)     # 4 variables per thread: at most 512 threads
+    with pytest.raises(NotImplementedError, match="two blocks per SM"):
+        dec.configure_launch(352, 1, 2, 2)     # two-shot groups keep one block per SM
+    with pytest.raises(ValueError, match="blocks_per_sm"):
+        dec.configure_launch(352, 1, 1, 3)
