@@ -9,9 +9,10 @@ iterations, gamma0 0.65, leg gammas U(-0.24, 0.66), stop_nconv 5), float32.
 The decoder measured is the learned one: the pre-iterations, the proposal
 network (for the shots they leave unconverged) and the relay legs with the
 learned strengths on legs 0-3 (LearnedRelayBPDecoder, gate=True), replayed
-as one CUDA graph per call.  The plain
-decoder (RelayBPDecoder.decode, seeded legs) decodes the same shots in the same
-run and is reported under "plain", with both logical error rates.
+as one CUDA graph per call.  The plain decoder (RelayBPDecoder.decode, seeded
+legs, also one CUDA-graph replay per call: cuda_graph=True) decodes the same
+shots in the same run and is reported under "plain", with both logical error
+rates.
 
   value  shots/s with the syndromes already in HBM (public decode() call on a
          device tensor), CUDA events on the launching stream, max over ranks;
@@ -109,7 +110,10 @@ class ClockSampler:
         self.rows: list[tuple[float, list[str]]] = []
         self._proc = None
 
-    def start(self):
+    def start(self, settle_s: float = 10.0):
+        """Start sampling and return once the first sample has arrived: nvidia-smi's start-up
+        (a one-time stall of about 15-70 ms of the running GPU work, seen as one long step) then
+        falls before the timed region instead of inside it."""
         try:
             self._proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
@@ -118,6 +122,10 @@ class ClockSampler:
             self._t.start()
         except OSError:
             self._proc = None
+            return self
+        deadline = time.time() + settle_s
+        while not self.rows and time.time() < deadline and self._proc.poll() is None:
+            time.sleep(0.01)
         return self
 
     def _read(self):
@@ -288,7 +296,8 @@ def main():
     from pelagos_b200 import autotune
 
     launch = tuple(int(x) for x in args.launch.split(",")) if args.launch else None
-    dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], launch=launch, **RELAY)
+    dec = RelayBPDecoder(w.H, w.priors, data_type=args.dtype, device=[local], launch=launch, cuda_graph=True,
+                         **RELAY)
     if launch is None:
         autotune.apply_default_shapes(dec)  # the shapes committed for this workload, if any
     params, meta = load_params(default_weights_path(WORKLOAD, P))
@@ -441,7 +450,8 @@ def main():
                       "logical_error_rate": p_ler,
                       "roofline": {"bound": "smem", "achieved": p_achieved, "peak": smem_peak, "unit": "GB/s",
                                    "frac": p_achieved / smem_peak, "shot_iterations_per_step": p_iters},
-                      "note": "the same shots through RelayBPDecoder.decode (seeded legs), same run"},
+                      "note": "the same shots through RelayBPDecoder.decode (seeded legs, one CUDA-graph "
+                              "replay per call like the learned decode), same run"},
             "step_ms": {"learned": {"min": min(l_steps), "median": float(np.median(l_steps)), "max": max(l_steps)},
                         "plain": {"min": min(p_steps), "median": float(np.median(p_steps)), "max": max(p_steps)}},
             "learned_over_plain": p_ms / ms_step,

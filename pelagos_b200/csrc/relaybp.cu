@@ -67,7 +67,7 @@ size_t msg_size(int t) { return t == RBP_MSG_F64 ? 8 : (t == RBP_MSG_F32 ? 4 : 2
 
 struct Layout {
   int off_chk_deg, off_llr, off_first, off_group0;
-  int g_msg, g_par, g_best, g_first, g_red, group_bytes;
+  int g_msg, g_par, g_best, g_first, g_red, g_s1, group_bytes;
 };
 
 // Rows of the check-slot layout: the slot count the kernel holds in registers
@@ -87,8 +87,10 @@ int slot_index_host(int j, int c, int C, int msg_type) {
   }
 }
 
-// Block-wide tables first, then one region per group.
-Layout make_layout(int C, int V, int rows, int msg_type, int group_threads) {
+// Block-wide tables first, then one region per group.  first_sums: the region also holds
+// the shot's first-pass sums, one accumulator per owned-variable slot (the one-shot
+// block-per-group kernel).
+Layout make_layout(int C, int V, int rows, int msg_type, int group_threads, bool first_sums = false) {
   Layout L{};
   int o = 0;
   L.off_chk_deg = o;
@@ -111,6 +113,16 @@ Layout make_layout(int C, int V, int rows, int msg_type, int group_threads) {
   q = align16(q + 4 * W);
   L.g_red = q;
   q = align16(q + 8 * (group_threads / 32 + 4));
+  L.g_s1 = q;
+  if (first_sums) {
+    int vpt = 16;  // owned variables per thread (vpt_for)
+    for (int v : rbpk::kVptChoices)
+      if ((long long)v * group_threads >= V) {
+        vpt = v;
+        break;
+      }
+    q = align16(q + (msg_type == RBP_MSG_F64 ? 8 : 4) * vpt * group_threads);
+  }
   L.group_bytes = q;
   return L;
 }
@@ -195,7 +207,7 @@ int choose_slots_launch(int C, int V, int slots, int vslots, int rows, int msg_t
                                  "degrees up to 16)"
                                : ": no block-per-group kernel for this degree / shape (check degrees "
                                  "above 16 run with several groups per block, one shot each)"));
-  const Layout L = make_layout(C, V, rows, msg_type, G);
+  const Layout L = make_layout(C, V, rows, msg_type, G, nshots == 1);
   const size_t smem = (size_t)L.off_group0 + (size_t)nshots * L.group_bytes;
   if (smem > max_smem)
     return fail(RBP_ERR_UNSUPPORTED, w + ": " + std::to_string(nshots) + " shots' state (" +
@@ -351,6 +363,7 @@ int launch_decode(const DevGraph& dgph, const rbp_params& p, const Layout& L, co
   a.g_best = L.g_best;
   a.g_first = L.g_first;
   a.g_red = L.g_red;
+  a.g_s1 = L.g_s1;
   const long long per_block = (long long)lc.groups * lc.nshots;  // shots a block decodes at once
   const long long need_blocks = (B + per_block - 1) / per_block;
   const int blocks = (int)std::min<long long>(lc.blocks, need_blocks);
@@ -495,7 +508,7 @@ int rbp_decoder_configure_kind(rbp_decoder* d, int32_t kind, int32_t group_threa
   const int rc = choose_launch(g->C, g->V, g->slots, g->vslots, d->rows, d->p.msg_type, G, groups_per_block,
                                d->max_smem, d->sm_count, &lc, "rbp_decoder_configure", nshots, minb);
   if (rc != RBP_OK) return rc;
-  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, G);
+  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, G, lc.slots_kernel && lc.nshots == 1);
   rbp_decoder::Shape sh;
   sh.kernel = lc.kernel;
   sh.vpt = vpt_for(g->V, G);
@@ -630,7 +643,7 @@ int rbp_decode(rbp_decoder* d, int64_t B, const rbp_batch* in, const rbp_outputs
   if (!dg.ok) return fail(RBP_ERR_CUDA, "rbp_decode: cannot select the CUDA device");
   // a launch that skips the relay legs runs at most pre_iter iterations per shot
   const rbp_decoder::Shape& sh = d->shape[in->skip_relay_legs ? 0 : 1];
-  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, sh.group_threads);
+  const Layout L = make_layout(g->C, g->V, d->rows, d->p.msg_type, sh.group_threads, sh.slots_kernel && sh.nshots == 1);
   const DevGraph dgph{g->C, g->V, g->E, g->slots, d->rows, g->vslots, g->chk_deg.p, g->chk_ptr.p, d->var_pos.p};
   const Launch lc{sh.kernel, sh.group_threads, sh.groups, sh.blocks, sh.nshots, sh.slots_kernel, sh.minb};
   return launch_decode(dgph, d->p, L, lc, d->llr.p, d->gamma_legs.p, d->alpha.p, d->queue.p, B, in,
@@ -734,6 +747,7 @@ int mixed_args(rbp_mixed* m, const int64_t* B, const rbp_batch* ins, const rbp_o
     a.g_best = L.g_best;
     a.g_first = L.g_first;
     a.g_red = L.g_red;
+    a.g_s1 = L.g_s1;
     work[i] = (double)B[i] * (double)g->E;
     total += work[i];
   }

@@ -220,6 +220,7 @@ struct DevArgs {
   int off_chk_deg, off_llr, off_first, off_group0, group_bytes;
   int first_table;               // 1: take each phase's first check pass from the block's table
   int g_msg, g_par, g_best, g_first, g_red;
+  int g_s1;                      // one-shot block-per-group kernel: the shot's first-pass sums
 };
 
 enum HardSrc { HARD_ZERO = 0, HARD_POST = 1, HARD_BEST = 2 };

@@ -85,6 +85,8 @@ struct SlotState {
   int claim;            // which red[1 + claim] entry the next claim writes
   int wsel;             // one-shot kernel: the next selection sums into red[0] (0) or red[4] (1)
   bool run, has_best, sel_seen, solved_pre, stopped;
+  bool s1_ok;           // one-shot kernel: the slot's first-pass sums belong to this shot
+  bool synced;          // the last iteration's test of the unsatisfied count was followed by a barrier
 };
 
 // One check row of one slot: min-sum (kernels.py:1052-1215) from the slot's
@@ -151,7 +153,8 @@ __device__ __forceinline__ void slot_check_row(M* msg, const M* first_tab, bool 
 template <typename M, int MAXDV, bool STORE = true>
 __device__ __forceinline__ uint32_t slot_var(M* msg, const uint32_t (&vp)[MAXDV], uint32_t dummy,
                                              typename MsgT<M>::A l0, typename MsgT<M>::A gam, int mix_mode,
-                                             typename MsgT<M>::A& post, typename MsgT<M>::A* lm_out = nullptr) {
+                                             typename MsgT<M>::A& post, typename MsgT<M>::A* lm_out = nullptr,
+                                             typename MsgT<M>::A* sum_out = nullptr) {
   using IO = MsgT<M>;
   using A = typename IO::A;
   const A lm = memory_mix<A>(mix_mode, gam, l0, post);
@@ -163,6 +166,7 @@ __device__ __forceinline__ uint32_t slot_var(M* msg, const uint32_t (&vp)[MAXDV]
     nv[j] = IO::ld(msg[vp[j]]);
     sum = (vp[j] != dummy) ? add_rn(sum, nv[j]) : sum;  // absent edges read the dummy slot
   }
+  if (sum_out) *sum_out = sum;
   const A pv = add_rn(lm, sum);
   post = pv;
   if constexpr (STORE) {
@@ -263,6 +267,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   auto first_of = [&](int s) { return reinterpret_cast<uint32_t*>(region0 + s * a.group_bytes + a.g_first); };
   auto red_of = [&](int s) { return reinterpret_cast<long long*>(region0 + s * a.group_bytes + a.g_red); };
   auto unsat_of = [&](int s) { return reinterpret_cast<int*>(red_of(s) + 3); };
+  auto s1_of = [&](int s) { return reinterpret_cast<A*>(region0 + s * a.group_bytes + a.g_s1); };
 
   // every slot's mis bits and unsatisfied count start at 0 (set-ups adjust them by differences)
 #pragma unroll
@@ -395,6 +400,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     x.hmask = 0u;
     x.hmask_sel = 0u;
     x.sel_seen = false;
+    x.s1_ok = false;
     x.has_best = has_best_raw != 0;
     x.stopped = false;
     // a shot resumed at leg 0 was solved by the pre-iterations if it found a solution there
@@ -615,25 +621,68 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   // collected in a mask and the few flips applied after the loop, so no branch splits the
   // loop body.  Ends with this thread's share of the unsatisfied-check count.
   // With DEFER the outgoing messages are not stored (see the one-shot schedule below);
-  // the memory mixes are kept in lm_keep for slot_var_store.
+  // the memory mixes are kept in lm_keep for slot_var_store.  A DEFER pass of a one-shot
+  // group whose first check pass came from the table also keeps each variable's sum of
+  // incoming messages in the slot's s1 array: those are the first-pass sums of every relay
+  // leg of the shot (the table and the shot's syndrome signs do not change between legs).
   A lm_keep[VPT];
   auto var_pass = [&](SlotState<A, VPT>& x, int s, auto defer) {
     constexpr bool DEFER = decltype(defer)::value;
     M* msg = msg_of(s);
+    A* s1 = s1_of(s);
+    const bool keep_sums = DEFER && NS == 1 && first_from_table;
     uint32_t hnew = 0u;
 #pragma unroll
     for (int kk = 0; kk < VPT; ++kk) {
       const int v = t + kk * G;
       const A l0 = x.llr_row ? (v < V ? A(__ldg(x.llr_row + v)) : A(1)) : (v < V ? A(s_llr[v]) : A(1));
+      A sum = A(0);
       hnew |= slot_var<M, MAXDV, !DEFER>(msg, vpos[kk], dummy, l0, x.gam[kk], a.mix_mode, x.post[kk],
-                                         DEFER ? &lm_keep[kk] : nullptr)
+                                         DEFER ? &lm_keep[kk] : nullptr, keep_sums ? &sum : nullptr)
               << kk;
+      if (keep_sums) s1[v] = sum;  // read back only by this thread (its own variables)
+    }
+    if (keep_sums) x.s1_ok = true;
+    const uint32_t flips = hnew ^ x.hmask;
+    x.hmask = hnew;
+    int dun = 0;
+    if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun, VC);
+    if (dun != 0) atomicAdd(unsat_of(s), dun);
+  };
+
+  // A relay leg's first iteration once the shot's first-pass sums are kept (one-shot groups):
+  // its check pass would copy the block's table with the shot's syndrome signs, the same
+  // messages as at every earlier leg's first iteration, and its variable pass would sum them
+  // in the same order again, so both are replaced by the kept sums.  The posterior, decision
+  // and memory mix are those var_pass computes; lm_keep serves the deferred stores.
+  auto var_pass_quick = [&](SlotState<A, VPT>& x, int s) {
+    const A* s1 = s1_of(s);
+    uint32_t hnew = 0u;
+#pragma unroll
+    for (int kk = 0; kk < VPT; ++kk) {
+      const int v = t + kk * G;
+      const A l0 = v < V ? A(s_llr[v]) : A(1);  // first pass from the table: no per-shot priors
+      const A lm = memory_mix<A>(a.mix_mode, x.gam[kk], l0, x.post[kk]);
+      lm_keep[kk] = lm;
+      const A pv = add_rn(lm, s1[v]);
+      x.post[kk] = pv;
+      hnew |= (pv <= A(0) ? 1u : 0u) << kk;
     }
     const uint32_t flips = hnew ^ x.hmask;
     x.hmask = hnew;
     int dun = 0;
     if (flips) slot_flips<M, MAXDC, VPT, MAXDV>(mis_of(s), vpos, dummy, flips, dun, VC);
     if (dun != 0) atomicAdd(unsat_of(s), dun);
+  };
+
+  // The first check pass from the table (the messages a quick first iteration skipped).
+  auto table_copy = [&](SlotState<A, VPT>& x, int s) {
+    M* msg = msg_of(s);
+    for (int k = 0; t + k * G < C; ++k) {
+      const int c = t + k * G;
+      slot_check_row<M, MAXDC>(msg, first_tab, true, c, C, s_chk_deg[c], (int)((x.synm >> k) & 1u), A(1), false,
+                               false, beta);
+    }
   };
 
   // After slot x's variable pass and the barrier: the iteration's convergence test,
@@ -680,9 +729,11 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
       x.iters += x.it;
       x.hard_src = HARD_BEST;
       x.run = false;
+      x.synced = true;  // a selection barrier followed every thread's read of the count
       return EV_PHASE_DONE;
     }
     x.hard_src = HARD_POST;
+    x.synced = false;
     if (x.it >= x.max_iter) {
       x.iters += x.max_iter;
       x.run = false;
@@ -702,6 +753,8 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     st[s].b = -1;  // no shot yet: the first EV_SHOT_DONE only claims
     st[s].has_best = false;
     st[s].stopped = false;
+    st[s].s1_ok = false;
+    st[s].synced = false;
     ev[s] = EV_SHOT_DONE;
   }
   if constexpr (NS == 1) {
@@ -709,18 +762,31 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
     while (true) {
       if (ev[0] != EV_NONE) events(st[0], 0, ev[0]);
       if (!st[0].run) break;
-      check_pass(st[0], 0);
-      __syncthreads();
       // A relay leg's first iteration usually converges (most legs of solved shots repeat
       // their solution), and then its outgoing messages are never read: the next leg restarts
       // them.  Those passes store them only once the iteration is known not to have converged.
       const bool defer = st[0].phase >= 0 && st[0].it == 0;
-      if (defer) var_pass(st[0], 0, std::true_type{});
-      else var_pass(st[0], 0, std::false_type{});
+      // From the shot's second leg in this launch on, that iteration needs no check pass.
+      const bool quick = defer && st[0].s1_ok;
+      if (quick) {
+        // the variable pass updates the unsatisfied count: every thread's read of it in the
+        // last iteration's test must come first (a convergence's selection ordered them)
+        if (!st[0].synced) __syncthreads();
+        var_pass_quick(st[0], 0);
+      } else {
+        check_pass(st[0], 0);
+        __syncthreads();
+        if (defer) var_pass(st[0], 0, std::true_type{});
+        else var_pass(st[0], 0, std::false_type{});
+      }
       __syncthreads();
       ev[0] = after_var(st[0], 0);
       if (defer && st[0].run) {
         M* msg = msg_of(0);
+        if (quick) {
+          table_copy(st[0], 0);  // the incoming messages the deferred stores re-sum
+          __syncthreads();
+        }
 #pragma unroll
         for (int kk = 0; kk < VPT; ++kk) slot_var_store<M, MAXDV>(msg, vpos[kk], dummy, lm_keep[kk]);
         __syncthreads();  // the next check pass reads them

@@ -94,3 +94,26 @@ def test_out_of_range_order_entries_are_skipped(shots):
     keep = np.ones(B, bool)
     keep[[3, 10]] = False
     np.testing.assert_array_equal(f[keep], ref["found_count"][keep])
+
+
+def test_cuda_graph_replay_equals_eager_decode(shots):
+    """cuda_graph=True: one graph replay per call gives the eager result for every batch of the
+    captured size (the input is copied in, the results cloned out), host syndromes included, and
+    a launch-shape change recaptures."""
+    w, syn = shots
+    eager = RelayBPDecoder(w.H, w.priors, **RELAY)
+    graphed = RelayBPDecoder(w.H, w.priors, cuda_graph=True, **RELAY)
+    a, b = syn[:4096].contiguous(), syn[4096:].contiguous()
+    want_a, want_b = _np(eager.decode(a)), _np(eager.decode(b))
+    got_a = graphed.decode(a)
+    got_b = graphed.decode(b.cpu())           # host syndromes: copied into the graph's input
+    got_a2 = _np(graphed.decode(a))
+    assert len(graphed._cuda_graphs) == 1
+    for got, want in ((_np(got_a), want_a), (_np(got_b), want_b), (got_a2, want_a)):
+        for k in KEYS:
+            np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+    graphed.configure_launch(704, 1, 1)
+    got = _np(graphed.decode(b))
+    assert graphed._cuda_graphs[4096][0][1] == (704, 1, 1, 0)
+    for k in KEYS:
+        np.testing.assert_array_equal(got[k], want_b[k], err_msg=k)
