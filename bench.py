@@ -61,11 +61,11 @@ METRIC = "shots/s on one B200 at matched logical error rate, learned vs plain Re
 CONFIG_NAME = "[[144,12,12]] BB phenomenological, 12 noisy + 1 perfect round, p=0.003, 65,536 shots"
 LEARNED_LEGS = 4
 # DRAM bytes (read + write) of the two decode-kernel launches of one learned decode, per shot: ncu
-# dram__bytes_read.sum + dram__bytes_write.sum on 16,384 shots of this workload
-# (python -m pelagos_b200.experiments decode-case --shots 16384 --learned), 361,716,736 B / 16,384.
-# At this size L2 keeps part of the saved states between the two launches; the states and I/O a
-# shot must move at any size come to about 26.6 KB.
-DECODE_DRAM_BYTES_PER_SHOT = 22077
+# dram__bytes_read.sum + dram__bytes_write.sum on 16,384 shots of this workload with the committed
+# kernel shape (python -m pelagos_b200.experiments decode-case --shots 16384 --learned
+# --launch 352,1,1,2), 369,452,032 B / 16,384.  At this size L2 keeps part of the saved states
+# between the two launches; the states and I/O a shot must move at any size come to about 26.6 KB.
+DECODE_DRAM_BYTES_PER_SHOT = 22550
 
 
 def algorithmic_bytes_per_shot_iteration(C: int, V: int, E: int, msg_bytes: int = 4) -> int:
