@@ -63,9 +63,9 @@ LEARNED_LEGS = 4
 # DRAM bytes (read + write) of the two decode-kernel launches of one learned decode, per shot: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum on 16,384 shots of this workload with the committed
 # kernel shape (python -m pelagos_b200.experiments decode-case --shots 16384 --learned
-# --launch 352,1,1,2), 369,452,032 B / 16,384.  At this size L2 keeps part of the saved states
+# --launch 448,1,1,2), 378,680,320 B / 16,384.  At this size L2 keeps part of the saved states
 # between the two launches; the states and I/O a shot must move at any size come to about 26.6 KB.
-DECODE_DRAM_BYTES_PER_SHOT = 22550
+DECODE_DRAM_BYTES_PER_SHOT = 23113
 
 
 def algorithmic_bytes_per_shot_iteration(C: int, V: int, E: int, msg_bytes: int = 4) -> int:
@@ -452,8 +452,10 @@ def main():
                                    "frac": p_achieved / smem_peak, "shot_iterations_per_step": p_iters},
                       "note": "the same shots through RelayBPDecoder.decode (seeded legs, one CUDA-graph "
                               "replay per call like the learned decode), same run"},
-            "step_ms": {"learned": {"min": min(l_steps), "median": float(np.median(l_steps)), "max": max(l_steps)},
-                        "plain": {"min": min(p_steps), "median": float(np.median(p_steps)), "max": max(p_steps)}},
+            "step_ms": {"learned": {"min": min(l_steps), "median": float(np.median(l_steps)), "max": max(l_steps),
+                                    "steps": [round(x, 3) for x in l_steps]},
+                        "plain": {"min": min(p_steps), "median": float(np.median(p_steps)), "max": max(p_steps),
+                                  "steps": [round(x, 3) for x in p_steps]}},
             "learned_over_plain": p_ms / ms_step,
             "phase_ms": {"decode_kernel": kern, "network_and_selection": float(np.mean(net_ms)),
                          "note": "eager runs of the same decode with events between its launches"},

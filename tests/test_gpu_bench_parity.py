@@ -7,8 +7,9 @@ decoded on the GPU and compared bit for bit with the CPU oracle:
 
 * the plain decoder (RelayBPDecoder.decode), with every kernel family (the
   block-per-group kernel with one and with two shots per group, the kernel
-  whose blocks hold several one-shot groups, and the benchmark's committed
-  shape: 352-thread one-shot groups at two resident blocks per SM);
+  whose blocks hold several one-shot groups, and one-shot groups at two
+  resident blocks per SM with 352 and with 448 threads, the latter the
+  benchmark's committed shape);
 * the gated learned decoder (LearnedRelayBPDecoder, gate=True) against the
   oracle's per-shot emulation of it: shots the pre-iterations solved run relay
   legs 0-3 at the constant top strength, the others run them with the
@@ -75,7 +76,7 @@ def plain_oracle(bench_batch):
     return _oracle_chunks(dec, syn, dec._leg_table(0))
 
 
-@pytest.mark.parametrize("launch", [(0, 1, 1), (0, 1, 2), (0, 0, 1), (352, 1, 1, 2)])
+@pytest.mark.parametrize("launch", [(0, 1, 1), (0, 1, 2), (0, 0, 1), (352, 1, 1, 2), (448, 1, 1, 2)])
 def test_plain_decode_of_the_bench_batch_matches_oracle(bench_batch, plain_oracle, launch):
     w, syn = bench_batch
     dec = RelayBPDecoder(w.H, w.priors, launch=launch, **RELAY)
@@ -86,7 +87,7 @@ def test_plain_decode_of_the_bench_batch_matches_oracle(bench_batch, plain_oracl
     assert got["iterations"].max() > 200
 
 
-@pytest.mark.parametrize("launch", [(0, 1, 1), (0, 1, 2), (0, 0, 1), (352, 1, 1, 2)])
+@pytest.mark.parametrize("launch", [(0, 1, 1), (0, 1, 2), (0, 0, 1), (352, 1, 1, 2), (448, 1, 1, 2)])
 def test_gated_learned_decode_of_the_bench_batch_matches_oracle_emulation(bench_batch, launch):
     from pelagos_b200.proposal import LearnedRelayBPDecoder, ProposalNet, default_weights_path, load_params
 
