@@ -16,6 +16,9 @@ rates.
 
   value  shots/s with the syndromes already in HBM (public decode() call on a
          device tensor), CUDA events on the launching stream, max over ranks;
+         a timed region in which one step took over twice the median step (a
+         stall outside the decode) is measured once more, and the line keeps
+         the first attempt's steps under "remeasured";
   e2e    shots/s through the streaming call decode_stream() over the K batches
          of pinned host syndromes: every batch's host->device copy of the
          syndromes and device->host copy of the result (errors, weight_fixed,
@@ -318,7 +321,7 @@ def main():
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    def timed_steps(fn):
+    def timed_once(fn):
         """K steps, each between its own pair of events on the launching stream; the L2 flush between
         steps (a 256 MB write) lies outside them.  The region is bracketed by a barrier and a device
         synchronisation on both sides; ms per step is the mean over steps, max over ranks.  Python's
@@ -345,10 +348,26 @@ def main():
         iters = sum(int(it.sum().item()) for it in step_iters) / args.steps
         return ms, per_step, o, iters
 
+    remeasured = {}
+
+    def timed_steps(fn, name):
+        """timed_once, measured once more when a step took over twice the median step on any rank
+        (a stall outside the decode: the kernels' own times do not change, see the launch list);
+        the line then reports the second attempt and keeps the first one's steps under
+        "remeasured".  Every rank takes the same decision (one reduction)."""
+        ms, per_step, o, iters = timed_once(fn)
+        worst = max_over_ranks(float(max(per_step) / np.median(per_step)), pg, dev)
+        if worst > 2.0:
+            remeasured[name] = {"reason": f"a step took {worst:.1f} x the median step",
+                                "first_attempt_ms_per_step": ms,
+                                "first_attempt_steps": [round(x, 3) for x in per_step]}
+            ms, per_step, o, iters = timed_once(fn)
+        return ms, per_step, o, iters
+
     clocks = ClockSampler(local).start()
     wall0 = time.time()
     # ---------------- the learned (gated) decode: the headline (CUDA-graph replay per call)
-    ms_step, l_steps, out, l_iters = timed_steps(lambda: learned.decode(syn_dev))
+    ms_step, l_steps, out, l_iters = timed_steps(lambda: learned.decode(syn_dev), "learned")
     # the same decode run eagerly with events between its launches, for the kernel times
     l_ev = []
     for _ in range(3):
@@ -360,7 +379,7 @@ def main():
     decode_ms = [e[0].elapsed_time(e[1]) + e[2].elapsed_time(e[3]) for e in l_ev]
     net_ms = [e[1].elapsed_time(e[2]) for e in l_ev]
     # ---------------- the plain decode of the same shots
-    p_ms, p_steps, p_out, p_iters = timed_steps(lambda: dec.decode(syn_dev))
+    p_ms, p_steps, p_out, p_iters = timed_steps(lambda: dec.decode(syn_dev), "plain")
     wall1 = time.time()
     clocks.stop()
     value = whole_job_shots_per_s(world, shots, ms_step)
@@ -457,6 +476,7 @@ def main():
                         "plain": {"min": min(p_steps), "median": float(np.median(p_steps)), "max": max(p_steps),
                                   "steps": [round(x, 3) for x in p_steps]}},
             "learned_over_plain": p_ms / ms_step,
+            "remeasured": remeasured,
             "phase_ms": {"decode_kernel": kern, "network_and_selection": float(np.mean(net_ms)),
                          "note": "eager runs of the same decode with events between its launches"},
             "e2e": {"value": e2e_value, "unit": "shots/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
