@@ -19,6 +19,17 @@
 // Each shot's arithmetic is exactly that of the one-shot kernel, so results
 // do not depend on which kernel or slot decodes a shot.
 //
+// Two resident blocks per SM (MINB 2, one shot per group): the same code with
+// half the register file per block, so two shots decode side by side on an SM
+// and one block's barrier and dependency waits become the other's issue slots.
+//
+// Relay legs' first iteration (one shot per group): a leg restarts the
+// messages, so its first check pass is the block's table with the shot's
+// syndrome signs, the same at every leg.  The shot's first leg in a launch
+// keeps each variable's sum of those messages (the s1 array of its slot);
+// later legs add the kept sum to the memory mix instead of running the check
+// pass and reloading the messages, which gives the same posterior bit for bit.
+//
 // Convergence test without a pass.  mis[c/32] bit c%32 holds (parity of check
 // c's current hard decisions) XOR (its syndrome bit): it starts as the syndrome
 // (all decisions start at 0) and the variable pass flips it with a shared

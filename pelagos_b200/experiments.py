@@ -121,7 +121,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["precision", "decode-case"])
     ap.add_argument("--shots", type=int, default=131072)
-    ap.add_argument("--launch", default="480,1", help="decode-case: G,groups kernel shape")
+    ap.add_argument("--launch", default="480,1",
+                    help="decode-case: G,groups[,shots_per_group[,blocks_per_sm]] kernel shape")
     ap.add_argument("--learned", action="store_true", help="decode-case: the learned (gated, eager) decode")
     ap.add_argument("--out", default=None)
     ap.add_argument("--dtypes", default="float64,float32,float16,bfloat16",
