@@ -130,7 +130,7 @@ RBP_API int rbp_decoder_configure(rbp_decoder* d, int32_t group_threads, int32_t
  * rbp_decoder_configure).  blocks_per_sm 2 selects the block-per-group kernel
  * compiled for two resident blocks per SM (groups_per_block 1 and
  * shots_per_group 1 only; half the register file per block, so
- * group_threads is at most 512 for up to 4 owned variables per thread, 480
+ * group_threads is at most 512 for up to 4 owned variables per thread, 448
  * for 6, 384 for 8 and 256 for 12 or 16): two shots decode side by side on an
  * SM, each at a longer iteration latency, which raises throughput and can
  * lengthen a batch whose slowest shot bounds it.  0 or 1: the kernels compiled

@@ -71,12 +71,12 @@ __host__ __device__ constexpr int max_slots_block_threads(int vpt, int ns = 2, i
 }
 
 // Largest block of the one-shot instantiations compiled for two resident
-// blocks per SM (MINB 2): each block gets half the register file, so the
-// owned-variable state is capped at 64 registers (VPT <= 6) or 80 (VPT 8).
-// Two shots then decode side by side on one SM with their own barriers, so
-// one block's barrier and dependency waits are filled by the other's work.
+// blocks per SM (MINB 2): each block gets half the register file, so a thread
+// has at most 64 registers (VPT <= 4), 72 (VPT 6), 80 (VPT 8) or 128.  Two
+// shots then decode side by side on one SM with their own barriers, so one
+// block's barrier and dependency waits are filled by the other's work.
 __host__ __device__ constexpr int max_slots_block_threads2(int vpt) {
-  return vpt <= 4 ? 512 : (vpt == 6 ? 480 : (vpt == 8 ? 384 : 256));
+  return vpt <= 4 ? 512 : (vpt == 6 ? 448 : (vpt == 8 ? 384 : 256));
 }
 
 template <typename A, int VPT>
