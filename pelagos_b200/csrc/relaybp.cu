@@ -88,8 +88,9 @@ int slot_index_host(int j, int c, int C, int msg_type) {
 }
 
 // Block-wide tables first, then one region per group.  first_sums: the region also holds
-// the shot's first-pass sums, one accumulator per owned-variable slot (the one-shot
-// block-per-group kernel).
+// the shot's first-pass sums and the memory mixes a relay leg's first iteration keeps for its
+// deferred stores, one accumulator each per owned-variable slot (the one-shot block-per-group
+// kernel).
 Layout make_layout(int C, int V, int rows, int msg_type, int group_threads, bool first_sums = false) {
   Layout L{};
   int o = 0;
@@ -121,7 +122,7 @@ Layout make_layout(int C, int V, int rows, int msg_type, int group_threads, bool
         vpt = v;
         break;
       }
-    q = align16(q + (msg_type == RBP_MSG_F64 ? 8 : 4) * vpt * group_threads);
+    q = align16(q + (msg_type == RBP_MSG_F64 ? 8 : 4) * 2 * vpt * group_threads);  // + memory mixes
   }
   L.group_bytes = q;
   return L;

@@ -632,11 +632,12 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   // collected in a mask and the few flips applied after the loop, so no branch splits the
   // loop body.  Ends with this thread's share of the unsatisfied-check count.
   // With DEFER the outgoing messages are not stored (see the one-shot schedule below);
-  // the memory mixes are kept in lm_keep for slot_var_store.  A DEFER pass of a one-shot
+  // the memory mixes are kept in the slot's shared lmk array (each thread's own entries, out
+  // of its registers) for slot_var_store.  A DEFER pass of a one-shot
   // group whose first check pass came from the table also keeps each variable's sum of
   // incoming messages in the slot's s1 array: those are the first-pass sums of every relay
   // leg of the shot (the table and the shot's syndrome signs do not change between legs).
-  A lm_keep[VPT];
+  auto lmk_of = [&](int s) { return s1_of(s) + VPT * G; };  // memory mixes kept for deferred stores
   auto var_pass = [&](SlotState<A, VPT>& x, int s, auto defer) {
     constexpr bool DEFER = decltype(defer)::value;
     M* msg = msg_of(s);
@@ -649,7 +650,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
       const A l0 = x.llr_row ? (v < V ? A(__ldg(x.llr_row + v)) : A(1)) : (v < V ? A(s_llr[v]) : A(1));
       A sum = A(0);
       hnew |= slot_var<M, MAXDV, !DEFER>(msg, vpos[kk], dummy, l0, x.gam[kk], a.mix_mode, x.post[kk],
-                                         DEFER ? &lm_keep[kk] : nullptr, keep_sums ? &sum : nullptr)
+                                         DEFER ? lmk_of(s) + v : nullptr, keep_sums ? &sum : nullptr)
               << kk;
       if (keep_sums) s1[v] = sum;  // read back only by this thread (its own variables)
     }
@@ -665,7 +666,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
   // its check pass would copy the block's table with the shot's syndrome signs, the same
   // messages as at every earlier leg's first iteration, and its variable pass would sum them
   // in the same order again, so both are replaced by the kept sums.  The posterior, decision
-  // and memory mix are those var_pass computes; lm_keep serves the deferred stores.
+  // and memory mix are those var_pass computes; lmk serves the deferred stores.
   auto var_pass_quick = [&](SlotState<A, VPT>& x, int s) {
     const A* s1 = s1_of(s);
     uint32_t hnew = 0u;
@@ -674,7 +675,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
       const int v = t + kk * G;
       const A l0 = v < V ? A(s_llr[v]) : A(1);  // first pass from the table: no per-shot priors
       const A lm = memory_mix<A>(a.mix_mode, x.gam[kk], l0, x.post[kk]);
-      lm_keep[kk] = lm;
+      lmk_of(s)[v] = lm;
       const A pv = add_rn(lm, s1[v]);
       x.post[kk] = pv;
       hnew |= (pv <= A(0) ? 1u : 0u) << kk;
@@ -799,7 +800,7 @@ __device__ __forceinline__ void run_slots(const DevGraph& g, const DevArgs& a, u
           __syncthreads();
         }
 #pragma unroll
-        for (int kk = 0; kk < VPT; ++kk) slot_var_store<M, MAXDV>(msg, vpos[kk], dummy, lm_keep[kk]);
+        for (int kk = 0; kk < VPT; ++kk) slot_var_store<M, MAXDV>(msg, vpos[kk], dummy, lmk_of(0)[t + kk * G]);
         __syncthreads();  // the next check pass reads them
       }
     }
